@@ -1,0 +1,218 @@
+"""Python host mirror of the reference's interface on top of the C ABI.
+
+Reference surface (same names, argument meaning and behaviour):
+
+* ``loadFullGraph(filename)``                       load.h:6, load.cpp:12-140
+* ``vHong(CSize, RSize, Fc, Fr, Bc, Br, t1, t2)``     scc.h:52, scc_WCC.cu:573
+* ``vSlota(CSize, RSize, Fc, Fr, Bc, Br, t1, t2)``    scc.h:50, scc_Coloring.cu:403
+* ``wHong(..., t1, t2, warpSize)``                  scc.h:51, scc_WCC.cu:53
+* ``wSlota(..., t1, t2, warpSize)``                 scc.h:49, scc_Coloring.cu:6
+
+The drivers print exactly what the reference prints (through the native
+library's stdout) and return the SCC count.  ``Engine`` adds what the
+reference never exposed: per-vertex canonical labels, device-resident
+inputs, counters and timings.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+from . import _native as N
+
+ALGOS = {"g": "vHong", "h": "vSlota", "x": "wHong", "y": "wSlota"}
+
+
+@dataclass
+class Graph:
+    """Host CSR in the reference layout (1-based; Fr/Br have V+2 entries)."""
+    V: int
+    E: int
+    Fr: np.ndarray
+    Fc: np.ndarray
+    Br: np.ndarray
+    Bc: np.ndarray
+    name: str = ""
+
+    def __post_init__(self):
+        for k in ("Fr", "Fc", "Br", "Bc"):
+            a = np.ascontiguousarray(getattr(self, k), dtype=np.uint32)
+            setattr(self, k, a)
+
+    @property
+    def nbytes(self) -> int:
+        return 4 * (2 * (self.V + 2) + 2 * self.E)
+
+
+@dataclass
+class Result:
+    labels: Optional[np.ndarray]      # V entries, labels[i] = min id of SCC of vertex i+1
+    num_sccs: int
+    num_trim1: int
+    num_trim2: int
+    num_pivot: int
+    stats: dict = field(default_factory=dict)
+
+
+def _ptr(a) -> int:
+    if a is None:
+        return 0
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    return int(a)
+
+
+def _algo_code(algo) -> int:
+    if isinstance(algo, str):
+        if algo in ALGOS:
+            return ord(algo)
+        inv = {v: k for k, v in ALGOS.items()}
+        if algo in inv:
+            return ord(inv[algo])
+        raise ValueError(f"unknown algorithm {algo!r}")
+    return int(algo)
+
+
+class Engine:
+    """An scc_context on one CUDA device."""
+
+    def __init__(self, device: int = 0):
+        self._lib = N.lib()
+        h = ctypes.c_void_p()
+        N.check(self._lib.scc_create(int(device), ctypes.byref(h)), "scc_create")
+        self._h = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.scc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):  # pragma: no cover - interpreter shutdown ordering
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_tuning(self, key: str, value: int) -> None:
+        N.check(self._lib.scc_set_tuning(self._h, key.encode(), int(value)), f"scc_set_tuning({key})")
+
+    def run(self, g: Graph, algo="h", t1=True, t2=True, warp=1, labels=True,
+            instrument=False, force=None) -> Result:
+        """Run on a host graph: the call copies the CSR in and the labels out."""
+        flags = (N.FLAG_TRIM1 if t1 else 0) | (N.FLAG_TRIM2 if t2 else 0)
+        flags |= N.FLAG_INSTRUMENT if instrument else 0
+        if force == "grid":
+            flags |= N.FLAG_FORCE_GRID
+        elif force == "block":
+            flags |= N.FLAG_FORCE_BLOCK
+        view = N.CsrView(g.V, g.E, _ptr(g.Fr), _ptr(g.Fc), _ptr(g.Br), _ptr(g.Bc))
+        out = np.zeros(max(g.V, 1), dtype=np.uint32) if labels else None
+        st = N.Stats()
+        rc = self._lib.scc_run(self._h, ctypes.byref(view), _algo_code(algo), flags, int(warp),
+                               _ptr(out), ctypes.byref(st), None)
+        N.check(rc, "scc_run")
+        return Result(out[:g.V] if labels else None, st.num_sccs, st.num_trim1, st.num_trim2,
+                      st.num_pivot, st.as_dict())
+
+    def run_device(self, V: int, E: int, Fr, Fc, Br, Bc, labels_out=None, algo="h", t1=True, t2=True,
+                   warp=1, instrument=False, stream=None, force=None) -> Result:
+        """Run on device-resident CSR (torch CUDA tensors or raw device pointers).
+
+        labels_out: device buffer of V uint32/int32 entries, or None.
+        stream: a cudaStream_t handle (int) or None for the engine's stream.
+        """
+        flags = N.FLAG_DEVICE | (N.FLAG_TRIM1 if t1 else 0) | (N.FLAG_TRIM2 if t2 else 0)
+        flags |= N.FLAG_INSTRUMENT if instrument else 0
+        if force == "grid":
+            flags |= N.FLAG_FORCE_GRID
+        elif force == "block":
+            flags |= N.FLAG_FORCE_BLOCK
+        view = N.CsrView(int(V), int(E), _ptr(Fr), _ptr(Fc), _ptr(Br), _ptr(Bc))
+        st = N.Stats()
+        rc = self._lib.scc_run(self._h, ctypes.byref(view), _algo_code(algo), flags, int(warp),
+                               _ptr(labels_out), ctypes.byref(st), stream)
+        N.check(rc, "scc_run")
+        return Result(None, st.num_sccs, st.num_trim1, st.num_trim2, st.num_pivot, st.as_dict())
+
+
+# ----------------------------------------------------------------------
+# graph files
+# ----------------------------------------------------------------------
+def _take_host_graph(hg: N.HostGraph, name: str = "") -> Graph:
+    V, E = int(hg.V), int(hg.E)
+    Fr = np.ctypeslib.as_array(hg.Fr, shape=(V + 2,)).copy()
+    Br = np.ctypeslib.as_array(hg.Br, shape=(V + 2,)).copy()
+    Fc = np.ctypeslib.as_array(hg.Fc, shape=(max(E, 1),))[:E].copy()
+    Bc = np.ctypeslib.as_array(hg.Bc, shape=(max(E, 1),))[:E].copy()
+    N.lib().scc_free_host_graph(ctypes.byref(hg))
+    return Graph(V, E, Fr, Fc, Br, Bc, name)
+
+
+def load_graph(path: str) -> Graph:
+    """GTgraph text (the reference's format) or the binary CSR format."""
+    hg = N.HostGraph()
+    N.check(N.lib().scc_load_graph(path.encode(), ctypes.byref(hg)), f"load {path}")
+    return _take_host_graph(hg, path)
+
+
+def graph_from_arcs(V: int, src, dst, name: str = "") -> Graph:
+    """Forward + reverse CSR from 1-based arcs, ordered as the reference loader orders them."""
+    src = np.ascontiguousarray(src, dtype=np.uint32)
+    dst = np.ascontiguousarray(dst, dtype=np.uint32)
+    hg = N.HostGraph()
+    N.check(N.lib().scc_graph_from_arcs(int(V), int(src.shape[0]), _ptr(src), _ptr(dst), ctypes.byref(hg)),
+            "scc_graph_from_arcs")
+    return _take_host_graph(hg, name)
+
+
+def save_binary(path: str, g: Graph) -> None:
+    hg = N.HostGraph(g.V, g.E, g.Fr.ctypes.data_as(N.u32p), g.Fc.ctypes.data_as(N.u32p),
+                     g.Br.ctypes.data_as(N.u32p), g.Bc.ctypes.data_as(N.u32p), None)
+    N.check(N.lib().scc_save_binary(path.encode(), ctypes.byref(hg)), f"save {path}")
+
+
+def loadFullGraph(filename: str):
+    """The reference's loader: returns (CSize, RSize, Fc, Fr, Bc, Br, Pr).
+
+    Pr (METIS partition ids, read only by the reference's detectSCC) is
+    zero-filled.
+    """
+    g = load_graph(filename)
+    return g.E, g.V, g.Fc, g.Fr, g.Bc, g.Br, np.zeros(g.V + 2, dtype=np.uint32)
+
+
+# ----------------------------------------------------------------------
+# reference drivers (print like the reference, return the count)
+# ----------------------------------------------------------------------
+def _reference_call(algo: str, CSize, RSize, Fc, Fr, Bc, Br, t1, t2, warpSize=1) -> int:
+    arrs = [np.ascontiguousarray(a, dtype=np.uint32) for a in (Fc, Fr, Bc, Br)]
+    n = ctypes.c_uint64(0)
+    rc = N.lib().scc_reference_call(ord(algo), int(CSize), int(RSize), _ptr(arrs[0]), _ptr(arrs[1]),
+                                    _ptr(arrs[2]), _ptr(arrs[3]), int(bool(t1)), int(bool(t2)),
+                                    int(warpSize), ctypes.byref(n))
+    if rc == 3:  # out of device memory: the reference throws this message
+        raise MemoryError("Error: Not enough memory on GPU\n")
+    N.check(rc, ALGOS[algo])
+    return int(n.value)
+
+
+def vHong(CSize, RSize, Fc, Fr, Bc, Br, t1=True, t2=True) -> int:
+    return _reference_call("g", CSize, RSize, Fc, Fr, Bc, Br, t1, t2)
+
+
+def vSlota(CSize, RSize, Fc, Fr, Bc, Br, t1=True, t2=True) -> int:
+    return _reference_call("h", CSize, RSize, Fc, Fr, Bc, Br, t1, t2)
+
+
+def wHong(CSize, RSize, Fc, Fr, Bc, Br, t1=True, t2=True, warpSize=1) -> int:
+    return _reference_call("x", CSize, RSize, Fc, Fr, Bc, Br, t1, t2, warpSize)
+
+
+def wSlota(CSize, RSize, Fc, Fr, Bc, Br, t1=True, t2=True, warpSize=1) -> int:
+    return _reference_call("y", CSize, RSize, Fc, Fr, Bc, Br, t1, t2, warpSize)

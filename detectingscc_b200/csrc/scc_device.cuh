@@ -1,0 +1,358 @@
+// Device-side building blocks of the B200 SCC engine.
+//
+// Vertex state is one 32-bit word per vertex (st[v]):
+//   bits  0..29  range name (FW-BW subproblem, Hong) or colour (Slota);
+//                0x3FFFFFFF marks a vertex whose SCC is already known
+//                (the reference's rangeSet tag, include/scc.h:36-37)
+//   bit   30     forward-visited  (FV, include/scc.h:24)
+//   bit   31     backward-visited (BV, include/scc.h:26)
+// so one gather per adjacency entry tells whether the neighbour is live, in
+// the same subproblem and unvisited.  The reference keeps uint8 tags plus a
+// uint32 range and reads both per edge (scc_kernels.cu:374-377).
+//
+// Every phase is written once against an execution policy:
+//   GridExec   all CTAs of a cooperative (co-resident) launch; passes end in
+//              a grid barrier whose wait is bounded by %globaltimer;
+//   BlockExec  one CTA; passes end in __syncthreads.
+// The plain path runs GridExec and drops to BlockExec on CTA 0 when the live
+// set gets small; the batched form runs one BlockExec per graph.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace sccb {
+
+constexpr uint32_t RMASK = 0x3FFFFFFFu;
+constexpr uint32_t DEAD = 0x3FFFFFFFu;
+constexpr uint32_t FVB = 0x40000000u;
+constexpr uint32_t BVB = 0x80000000u;
+constexpr uint32_t FULL = 0xFFFFFFFFu;
+constexpr uint32_t MAX_V = 0x0FFFFFFEu;   // 4V+3 split names must stay below DEAD
+
+// Load-balancing constants of the frontier expansion: a frontier vertex
+// whose degree exceeds HEAVY_T is cut into CH-edge chunks that the next pass
+// spreads over all warps.
+constexpr uint32_t HEAVY_T = 256;
+constexpr uint32_t CH = 512;
+
+// error codes shared with the host (include/scc_b200.h)
+constexpr int E_OVERFLOW = 20;
+constexpr int E_NOT_CONVERGED = 21;
+constexpr int E_TIMEOUT = 22;
+constexpr int E_BAD_GRAPH = 23;
+
+enum { C_FQ = 0, C_BQ = 1, C_FH = 2, C_BH = 3, C_LIST = 4, C_AUX = 5, NCNT = 8 };
+
+struct __align__(128) Ctl {
+    unsigned bar_count; unsigned _p0[31];
+    unsigned bar_word; unsigned _p1[31];          // generation (bits 0..30) | error (bit 31)
+    int error; int where; unsigned _p2[30];
+    unsigned lc[3][NCNT]; unsigned _p3[8];         // per-pass counters, 3-slot ring
+    unsigned long long n_trim1, n_trim2, n_pivot;
+    unsigned long long t_edges, t_verts;           // instrumented work counters
+    unsigned passes, outer;                        // passes run, peels / iterations
+    unsigned long long timeout_ns;
+    unsigned tail_pass;                            // pass at which CTA 0 took over (0 = never)
+    unsigned nlive_tail;
+};
+
+struct Graph {
+    uint32_t V, E;
+    const uint32_t *__restrict__ Fr, *__restrict__ Fc, *__restrict__ Br, *__restrict__ Bc;
+};
+
+struct Work {
+    uint32_t *st, *label, *stamp;
+    uint32_t *L[2];
+    uint32_t *Q[2][2];          // [direction][parity]
+    uint2 *H[2][2];             // heavy chunks (vertex, chunk) [direction][parity]
+    uint32_t hcap;
+    unsigned long long *pivkey; // Hong: 4V+4 slots; Slota: 1
+    Ctl *ctl;
+};
+
+__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
+__device__ __forceinline__ unsigned long long gtimer()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ unsigned vld(const unsigned *p) { return *(const volatile unsigned *)p; }
+__device__ __forceinline__ void set_error(Ctl *c, int code, int where)
+{
+    if (atomicCAS(&c->error, 0, code) == 0) c->where = where;
+}
+
+// Adjacency ids must lie in [1, V].  An id outside that range is reported
+// as a malformed graph and treated as vertex 0, which is permanently dead,
+// so no state array is ever indexed out of bounds.
+__device__ __forceinline__ uint32_t guard_id(uint32_t x, uint32_t V, Ctl *c)
+{
+    if (x - 1u >= V) {
+        set_error(c, E_BAD_GRAPH, 60);
+        return 0u;
+    }
+    return x;
+}
+
+// ---------------------------------------------------------------------
+// execution policies
+// ---------------------------------------------------------------------
+template <bool INSTR>
+struct GridExec {
+    static constexpr bool instr = INSTR;
+    static constexpr bool grid = true;
+    Ctl *ctl;
+    unsigned gl;   // pass counter, identical in every thread
+    __device__ __forceinline__ unsigned tid() const { return blockIdx.x * blockDim.x + threadIdx.x; }
+    __device__ __forceinline__ unsigned nthr() const { return gridDim.x * blockDim.x; }
+    __device__ __forceinline__ unsigned wid() const { return tid() >> 5; }
+    __device__ __forceinline__ unsigned nwarps() const { return nthr() >> 5; }
+    __device__ __forceinline__ bool leader() const { return blockIdx.x == 0 && threadIdx.x == 0; }
+
+    // Grid barrier.  The releasing CTA folds the error flag into the
+    // generation word so that every CTA takes the same decision; a waiter
+    // gives up after ctl->timeout_ns and reports E_TIMEOUT.
+    __device__ bool sync()
+    {
+        __shared__ unsigned s_word;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned w0 = vld(&ctl->bar_word);
+            __threadfence();
+            unsigned arrived = atomicAdd(&ctl->bar_count, 1u);
+            unsigned res;
+            if (arrived == gridDim.x - 1) {
+                atomicExch(&ctl->bar_count, 0u);
+                int err = *(volatile int *)&ctl->error;
+                res = ((w0 + 1u) & 0x7FFFFFFFu) | (err ? 0x80000000u : 0u);
+                __threadfence();
+                atomicExch(&ctl->bar_word, res);
+            } else {
+                unsigned long long t0 = gtimer();
+                for (;;) {
+                    res = vld(&ctl->bar_word);
+                    if ((res & 0x7FFFFFFFu) != (w0 & 0x7FFFFFFFu)) break;
+                    if (gtimer() - t0 > ctl->timeout_ns) {
+                        set_error(ctl, E_TIMEOUT, 1000);
+                        res = 0x80000000u;
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+            }
+            __threadfence();
+            s_word = res;
+        }
+        __syncthreads();
+        return !(s_word & 0x80000000u);
+    }
+};
+
+template <bool INSTR>
+struct BlockExec {
+    static constexpr bool instr = INSTR;
+    static constexpr bool grid = false;
+    Ctl *ctl;
+    unsigned gl;
+    __device__ __forceinline__ unsigned tid() const { return threadIdx.x; }
+    __device__ __forceinline__ unsigned nthr() const { return blockDim.x; }
+    __device__ __forceinline__ unsigned wid() const { return threadIdx.x >> 5; }
+    __device__ __forceinline__ unsigned nwarps() const { return blockDim.x >> 5; }
+    __device__ __forceinline__ bool leader() const { return threadIdx.x == 0; }
+    __device__ bool sync()
+    {
+        __shared__ int s_err;
+        __syncthreads();
+        if (threadIdx.x == 0) s_err = *(volatile int *)&ctl->error;
+        __syncthreads();
+        return s_err == 0;
+    }
+};
+
+// One pass: clear the counters the pass after next will push into, run the
+// body with (cur, nxt) counter slots, then the barrier.  A pass pushes into
+// counter slot gl%3 and buffer parity gl&1; the following pass reads them as
+// its "current" slot (gl+2)%3 and parity (gl+1)&1.
+template <class Ex, class F>
+__device__ __forceinline__ bool run_pass(Ex &ex, F &&body)
+{
+    const unsigned nxt = ex.gl % 3u, clr = (ex.gl + 1u) % 3u, cur = (ex.gl + 2u) % 3u;
+    if (ex.leader()) {
+#pragma unroll
+        for (int i = 0; i < NCNT; i++) ex.ctl->lc[clr][i] = 0u;
+    }
+    body(cur, nxt);
+    bool ok = ex.sync();
+    ex.gl++;
+    return ok;
+}
+
+// Counter value pushed by the pass that just finished.
+template <class Ex>
+__device__ __forceinline__ unsigned last_count(const Ex &ex, int which)
+{
+    return vld(&ex.ctl->lc[(ex.gl + 2u) % 3u][which]);
+}
+
+// ---------------------------------------------------------------------
+// warp primitives
+// ---------------------------------------------------------------------
+
+// Warp-aggregated append (ballot + one atomicAdd per warp): the frontier
+// compaction.  All 32 lanes must call it.
+__device__ __forceinline__ void warp_push(bool pred, uint32_t val, uint32_t *q, unsigned *cnt,
+                                          uint32_t cap, Ctl *ctl, int where)
+{
+    unsigned m = __ballot_sync(FULL, pred);
+    if (m == 0u) return;
+    unsigned lane = lane_id();
+    unsigned ld = __ffs(m) - 1u;
+    unsigned base = 0;
+    if (lane == ld) base = atomicAdd(cnt, (unsigned)__popc(m));
+    base = __shfl_sync(FULL, base, ld);
+    if (pred) {
+        unsigned pos = base + __popc(m & ((1u << lane) - 1u));
+        if (pos < cap) q[pos] = val;
+        else set_error(ctl, E_OVERFLOW, where);
+    }
+}
+
+__device__ __forceinline__ unsigned warp_incl_scan(unsigned x)
+{
+    unsigned lane = lane_id();
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        unsigned y = __shfl_up_sync(FULL, x, o);
+        if (lane >= (unsigned)o) x += y;
+    }
+    return x;
+}
+
+// Append nch chunk descriptors (v, 0..nch-1) per lane.  All lanes call.
+__device__ __forceinline__ void warp_push_chunks(uint32_t v, uint32_t nch, uint2 *hq, unsigned *hcnt,
+                                                 uint32_t hcap, Ctl *ctl)
+{
+    unsigned incl = warp_incl_scan(nch);
+    unsigned total = __shfl_sync(FULL, incl, 31);
+    if (total == 0u) return;
+    unsigned base = 0;
+    if (lane_id() == 0) base = atomicAdd(hcnt, total);
+    base = __shfl_sync(FULL, base, 0);
+    unsigned pos = base + incl - nch;
+    if (pos + nch > hcap) { if (nch) set_error(ctl, E_OVERFLOW, 2); return; }
+    for (uint32_t c = 0; c < nch; c++) hq[pos + c] = make_uint2(v, c);
+}
+
+// First pusher of u for pass tag wins (stamp dedup of work lists).
+__device__ __forceinline__ bool stamp_claim(uint32_t *stamp, uint32_t u, uint32_t tag)
+{
+    if (stamp[u] >= tag) return false;
+    return atomicMax(&stamp[u], tag) < tag;
+}
+
+// Load-balanced expansion of up to 32 adjacency lists held one per lane
+// (merge-path style): the warp walks the concatenation of the lists 32
+// entries at a time, each lane finds its owner by a 5-step binary search
+// over the exclusive scan of the degrees.  fn(valid, neighbour, aux_of_owner)
+// is called by all lanes on every step.  Degrees must be <= HEAVY_T.
+template <class Fn>
+__device__ __forceinline__ unsigned lbs_expand(uint32_t beg, uint32_t deg, uint32_t aux,
+                                               const uint32_t *__restrict__ C, Fn &&fn)
+{
+    unsigned incl = warp_incl_scan(deg);
+    unsigned total = __shfl_sync(FULL, incl, 31);
+    unsigned excl = incl - deg;
+    unsigned lane = lane_id();
+    for (unsigned base = 0; base < total; base += 32u) {
+        unsigned e = base + lane;
+        unsigned lo = 0;
+#pragma unroll
+        for (unsigned step = 16; step >= 1; step >>= 1) {
+            unsigned cand = lo + step;
+            unsigned x = __shfl_sync(FULL, excl, cand & 31u);
+            if (cand < 32u && x <= e) lo = cand;
+        }
+        unsigned ex_o = __shfl_sync(FULL, excl, lo);
+        unsigned beg_o = __shfl_sync(FULL, beg, lo);
+        unsigned aux_o = __shfl_sync(FULL, aux, lo);
+        bool valid = e < total;
+        uint32_t nbr = valid ? __ldg(&C[beg_o + (e - ex_o)]) : 0u;
+        fn(valid, nbr, aux_o);
+    }
+    return total;
+}
+
+// Virtual-warp expansion: groups of W = 1 << lw lanes share one vertex and
+// stride over its adjacency (the reference's fwd_warp/bwd_warp schedule,
+// include/scc_kernels.h:46-105).  Returns the entries scanned by the warp.
+template <class Fn>
+__device__ __forceinline__ unsigned vw_expand(uint32_t beg, uint32_t deg, uint32_t aux, unsigned lw,
+                                              const uint32_t *__restrict__ C, Fn &&fn)
+{
+    unsigned W = 1u << lw;
+    unsigned sub = lane_id() & (W - 1u);
+    unsigned maxd = __reduce_max_sync(FULL, deg);
+    for (unsigned base = 0; base < maxd; base += W) {
+        unsigned k = base + sub;
+        bool valid = k < deg;
+        uint32_t nbr = valid ? __ldg(&C[beg + k]) : 0u;
+        fn(valid, nbr, aux);
+    }
+    unsigned own = (sub == 0u) ? deg : 0u;
+    return __reduce_add_sync(FULL, own);
+}
+
+// 64-bit max of a pivot key over the warp, then the CTA; the CTA's thread 0
+// performs one atomicMax.  Called by every thread of the CTA.
+__device__ __forceinline__ void block_max_atomic(unsigned long long key, unsigned long long *dst)
+{
+    __shared__ unsigned long long s_red[32];
+    unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+    unsigned mhi = __reduce_max_sync(FULL, hi);
+    unsigned mlo = __reduce_max_sync(FULL, hi == mhi ? lo : 0u);
+    unsigned long long wk = ((unsigned long long)mhi << 32) | mlo;
+    unsigned w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (lane_id() == 0) s_red[w] = wk;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long m = 0;
+        for (unsigned i = 0; i < nw; i++) m = s_red[i] > m ? s_red[i] : m;
+        if (m && m > *(volatile unsigned long long *)dst) atomicMax(dst, m);
+    }
+    __syncthreads();
+}
+
+// Pivot key (scc_kernels.cu:643-656): uint32 product of full-graph out- and
+// in-degree, larger wins; ties go to the smaller id.  Never 0 for v <= MAX_V.
+__device__ __forceinline__ unsigned long long pivot_key(const Graph &g, uint32_t v)
+{
+    uint32_t prod = (__ldg(&g.Fr[v + 1]) - __ldg(&g.Fr[v])) * (__ldg(&g.Br[v + 1]) - __ldg(&g.Br[v]));
+    return ((unsigned long long)prod << 32) | (unsigned long long)(0xFFFFFFFFu - v);
+}
+__device__ __forceinline__ uint32_t key_vertex(unsigned long long k) { return 0xFFFFFFFFu - (uint32_t)k; }
+
+// Range names after a FW-BW split: three fresh names per pivot.  The
+// reference uses 3*range + FV + 2*BV (scc_kernels.cu:138), which wraps.
+__device__ __forceinline__ uint32_t split_name(uint32_t V, uint32_t p, uint32_t s)
+{
+    return (V + 1u) + 3u * p + ((s & FVB) ? 1u : 0u) + ((s & BVB) ? 2u : 0u);
+}
+
+// Per-range atomicMax of pivot keys with warp aggregation over lanes that
+// share a range (match.any + redux) and a read before the atomic.
+__device__ __forceinline__ void range_max_atomic(bool valid, uint32_t r, unsigned long long key,
+                                                 unsigned long long *pivkey)
+{
+    unsigned grp = __match_any_sync(FULL, valid ? r : 0xFFFFFFFFu);
+    unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+    unsigned mhi = __reduce_max_sync(grp, hi);
+    unsigned mlo = __reduce_max_sync(grp, hi == mhi ? lo : 0u);
+    if (valid && lane_id() == (unsigned)(__ffs(grp) - 1)) {
+        unsigned long long k = ((unsigned long long)mhi << 32) | mlo;
+        if (k > *(volatile unsigned long long *)&pivkey[r]) atomicMax(&pivkey[r], k);
+    }
+}
+
+}  // namespace sccb

@@ -1,0 +1,424 @@
+// Kernels and host side of the C ABI (include/scc_b200.h).
+//
+// One scc_run = (optional H2D copies) -> offset validation -> one SCC
+// launch (cooperative whole-GPU persistent kernel, or one CTA for small
+// graphs) -> two canonicalisation kernels -> (optional D2H of labels) -> one
+// D2H of the control block.  The reference instead issues one launch plus
+// one or two blocking 1-byte copies per BFS level and per propagation sweep
+// (e.g. scc_WCC.cu:880-885).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <new>
+
+#include "../../include/scc_b200.h"
+#include "scc_phases.cuh"
+#include "scc_internal.h"
+
+using namespace sccb;
+
+#define SCC_VERSION_STRING "scc_b200 0.1 (sm_100a)"
+
+struct Params {
+    Graph g;
+    Work w;
+    int t1, t2, lw;
+    uint32_t tail_n;
+};
+
+// ---------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------
+constexpr int GRID_THREADS = 512;
+constexpr int BLOCK_THREADS = 1024;
+
+template <bool INSTR, bool HONG>
+__global__ void __launch_bounds__(GRID_THREADS, 2) k_scc_grid(Params p)
+{
+    if (*(volatile int *)&p.w.ctl->error) return;
+    GridExec<INSTR> ex{p.w.ctl, 0u};
+    Carry cy{0u, 0u, 0u};
+    int rc = HONG ? hong_front(ex, p.g, p.w, p.t1, p.t2, p.lw, cy) : slota_front(ex, p.g, p.w, p.t1, p.lw, cy);
+    if (rc == RUN_DONE) rc = HONG ? hong_loop(ex, p.g, p.w, cy, p.tail_n) : slota_peels(ex, p.g, p.w, cy, p.tail_n);
+    if (rc == RUN_SWITCH) {
+        // the live set is small: CTA 0 finishes alone with block barriers
+        if (blockIdx.x != 0) return;
+        if (threadIdx.x == 0) { p.w.ctl->tail_pass = cy.gl; p.w.ctl->nlive_tail = cy.nL; }
+        BlockExec<INSTR> bx{p.w.ctl, cy.gl};
+        if (HONG) hong_loop(bx, p.g, p.w, cy, 0u);
+        else slota_peels(bx, p.g, p.w, cy, 0u);
+        if (threadIdx.x == 0) p.w.ctl->passes = bx.gl;
+        return;
+    }
+    if (ex.leader()) p.w.ctl->passes = ex.gl;
+}
+
+template <bool INSTR, bool HONG>
+__global__ void __launch_bounds__(BLOCK_THREADS, 1) k_scc_block(Params p)
+{
+    if (*(volatile int *)&p.w.ctl->error) return;
+    BlockExec<INSTR> ex{p.w.ctl, 0u};
+    Carry cy{0u, 0u, 0u};
+    int rc = HONG ? hong_front(ex, p.g, p.w, p.t1, p.t2, p.lw, cy) : slota_front(ex, p.g, p.w, p.t1, p.lw, cy);
+    if (rc == RUN_DONE) {
+        if (HONG) hong_loop(ex, p.g, p.w, cy, 0u);
+        else slota_peels(ex, p.g, p.w, cy, 0u);
+    }
+    if (threadIdx.x == 0) p.w.ctl->passes = ex.gl;
+}
+
+// Offsets must be the reference layout: Fr[0] = Fr[1] = 0, non-decreasing,
+// Fr[V+1] = E (load.cpp:55-77); same for Br.  Column ids are checked where
+// they are read (guard_id).
+__global__ void k_validate(Graph g, Ctl *ctl)
+{
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, n = gridDim.x * blockDim.x;
+    for (uint32_t i = tid; i <= g.V; i += n) {
+        if (__ldg(&g.Fr[i]) > __ldg(&g.Fr[i + 1]) || __ldg(&g.Br[i]) > __ldg(&g.Br[i + 1]))
+            set_error(ctl, E_BAD_GRAPH, 61);
+    }
+    if (tid == 0) {
+        if (g.Fr[0] != 0u || g.Fr[1] != 0u || g.Br[0] != 0u || g.Br[1] != 0u || g.Fr[g.V + 1] != g.E ||
+            g.Br[g.V + 1] != g.E)
+            set_error(ctl, E_BAD_GRAPH, 62);
+    }
+}
+
+// Canonical labels: the smallest vertex id of each representative group.
+// st[] is all DEAD (0x3FFFFFFF) once every vertex is assigned, so it serves
+// as the min-table.
+__global__ void k_canon_min(const uint32_t *__restrict__ label, uint32_t *canon, uint32_t V)
+{
+    const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t base = wid * 32u; base < V; base += nw * 32u) {
+        uint32_t v = base + lane_id() + 1u;
+        bool valid = v <= V;
+        uint32_t l = valid ? label[v] : 0xFFFFFFFFu;
+        unsigned grp = __match_any_sync(FULL, l);
+        uint32_t mn = __reduce_min_sync(grp, valid ? v : 0xFFFFFFFFu);
+        if (valid && lane_id() == (unsigned)(__ffs(grp) - 1) && l <= V && mn < canon[l]) atomicMin(&canon[l], mn);
+    }
+}
+
+__global__ void k_canon_write(const uint32_t *__restrict__ label, const uint32_t *__restrict__ canon,
+                              uint32_t *__restrict__ out, uint32_t V)
+{
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, n = gridDim.x * blockDim.x;
+    for (uint32_t v = tid + 1u; v <= V; v += n) {
+        uint32_t l = label[v];
+        out[v - 1u] = l <= V ? canon[l] : 0u;
+    }
+}
+
+// ---------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------
+namespace {
+
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+int cuda_status(cudaError_t e)
+{
+    if (e == cudaSuccess) return SCC_OK;
+    if (e == cudaErrorMemoryAllocation) return SCC_ERR_OOM;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver || e == cudaErrorNoKernelImageForDevice ||
+        e == cudaErrorInvalidDevice)
+        return SCC_ERR_NO_DEVICE;
+    return SCC_ERR_CUDA;
+}
+
+#define CK(call)                                  \
+    do {                                          \
+        cudaError_t _e = (call);                  \
+        if (_e != cudaSuccess) {                  \
+            ctx->last_cuda_error = (int)_e;       \
+            return cuda_status(_e);               \
+        }                                         \
+    } while (0)
+
+template <bool INSTR, bool HONG>
+void *grid_kernel_ptr() { return (void *)k_scc_grid<INSTR, HONG>; }
+template <bool INSTR, bool HONG>
+void *block_kernel_ptr() { return (void *)k_scc_block<INSTR, HONG>; }
+
+void *pick_grid(bool instr, bool hong)
+{
+    if (instr) return hong ? grid_kernel_ptr<true, true>() : grid_kernel_ptr<true, false>();
+    return hong ? grid_kernel_ptr<false, true>() : grid_kernel_ptr<false, false>();
+}
+void *pick_block(bool instr, bool hong)
+{
+    if (instr) return hong ? block_kernel_ptr<true, true>() : block_kernel_ptr<true, false>();
+    return hong ? block_kernel_ptr<false, true>() : block_kernel_ptr<false, false>();
+}
+
+}  // namespace
+
+int scc_ctx_reserve(scc_context *ctx, uint32_t V, uint32_t E)
+{
+    const size_t hcap = (size_t)E / CH + (size_t)E / HEAVY_T + 64;
+    const size_t n1 = (size_t)V + 1;
+    size_t need = 0;
+    auto take = [&](size_t bytes) { size_t off = need; need = align_up(need + bytes, 256); return off; };
+    size_t o_st = take(n1 * 4), o_label = take(n1 * 4), o_stamp = take(n1 * 4);
+    size_t o_L0 = take(n1 * 4), o_L1 = take(n1 * 4);
+    size_t o_Q[4], o_H[4];
+    for (int i = 0; i < 4; i++) o_Q[i] = take(n1 * 4);
+    for (int i = 0; i < 4; i++) o_H[i] = take(hcap * sizeof(uint2));
+    size_t o_piv = take((4 * n1 + 8) * 8);
+    size_t o_ctl = take(sizeof(Ctl));
+    if (need > ctx->ws_bytes) {
+        if (ctx->ws) cudaFree(ctx->ws);
+        ctx->ws = nullptr;
+        ctx->ws_bytes = 0;
+        cudaError_t e = cudaMalloc((void **)&ctx->ws, need);
+        if (e != cudaSuccess) { ctx->last_cuda_error = (int)e; cudaGetLastError(); return SCC_ERR_OOM; }
+        ctx->ws_bytes = need;
+    }
+    char *b = ctx->ws;
+    Work &w = ctx->work;
+    w.st = (uint32_t *)(b + o_st);
+    w.label = (uint32_t *)(b + o_label);
+    w.stamp = (uint32_t *)(b + o_stamp);
+    w.L[0] = (uint32_t *)(b + o_L0);
+    w.L[1] = (uint32_t *)(b + o_L1);
+    w.Q[0][0] = (uint32_t *)(b + o_Q[0]);
+    w.Q[0][1] = (uint32_t *)(b + o_Q[1]);
+    w.Q[1][0] = (uint32_t *)(b + o_Q[2]);
+    w.Q[1][1] = (uint32_t *)(b + o_Q[3]);
+    w.H[0][0] = (uint2 *)(b + o_H[0]);
+    w.H[0][1] = (uint2 *)(b + o_H[1]);
+    w.H[1][0] = (uint2 *)(b + o_H[2]);
+    w.H[1][1] = (uint2 *)(b + o_H[3]);
+    w.hcap = (uint32_t)std::min<size_t>(hcap, 0xFFFFFFFFu);
+    w.pivkey = (unsigned long long *)(b + o_piv);
+    w.ctl = (Ctl *)(b + o_ctl);
+    return SCC_OK;
+}
+
+static int ensure_csr_mirror(scc_context *ctx, uint32_t V, uint32_t E)
+{
+    size_t nv = (size_t)V + 2, ne = std::max<size_t>(E, 1);
+    if (nv > ctx->capV) {
+        cudaFree(ctx->dFr); cudaFree(ctx->dBr); cudaFree(ctx->dlab);
+        ctx->dFr = ctx->dBr = ctx->dlab = nullptr; ctx->capV = 0;
+        CK(cudaMalloc((void **)&ctx->dFr, nv * 4));
+        CK(cudaMalloc((void **)&ctx->dBr, nv * 4));
+        CK(cudaMalloc((void **)&ctx->dlab, nv * 4));
+        ctx->capV = nv;
+    }
+    if (ne > ctx->capE) {
+        cudaFree(ctx->dFc); cudaFree(ctx->dBc);
+        ctx->dFc = ctx->dBc = nullptr; ctx->capE = 0;
+        CK(cudaMalloc((void **)&ctx->dFc, ne * 4));
+        CK(cudaMalloc((void **)&ctx->dBc, ne * 4));
+        ctx->capE = ne;
+    }
+    return SCC_OK;
+}
+
+extern "C" const char *scc_version(void) { return SCC_VERSION_STRING; }
+
+extern "C" const char *scc_status_string(int s)
+{
+    switch (s) {
+    case SCC_OK: return "ok";
+    case SCC_ERR_INVALID_ARG: return "invalid argument";
+    case SCC_ERR_CUDA: return "CUDA runtime error";
+    case SCC_ERR_OOM: return "Error: Not enough memory on GPU";
+    case SCC_ERR_TOO_LARGE: return "graph too large (V above 2^28 - 2)";
+    case SCC_ERR_NO_DEVICE: return "no usable CUDA device (sm_100a required)";
+    case SCC_ERR_BUDGET: return "device memory budget exceeded";
+    case SCC_ERR_IO: return "Error Reading graph file";
+    case SCC_ERR_OVERFLOW: return "internal work list overflow";
+    case SCC_ERR_NOT_CONVERGED: return "iteration cap reached before convergence";
+    case SCC_ERR_TIMEOUT: return "grid barrier wait timed out";
+    case SCC_ERR_BAD_GRAPH: return "malformed CSR (offsets or vertex ids)";
+    default: return "unknown status";
+    }
+}
+
+extern "C" int scc_create(int device, scc_context **out)
+{
+    if (!out) return SCC_ERR_INVALID_ARG;
+    *out = nullptr;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n <= 0) { cudaGetLastError(); return SCC_ERR_NO_DEVICE; }
+    if (device < 0 || device >= n) return SCC_ERR_NO_DEVICE;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return SCC_ERR_NO_DEVICE;
+    if (prop.major != 10) return SCC_ERR_NO_DEVICE;
+    scc_context *ctx = new (std::nothrow) scc_context();
+    if (!ctx) return SCC_ERR_OOM;
+    ctx->device = device;
+    ctx->nsm = prop.multiProcessorCount;
+    ctx->coop = prop.cooperativeLaunch;
+    if (cudaSetDevice(device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMallocHost((void **)&ctx->hctl, sizeof(Ctl)) != cudaSuccess ||
+        cudaEventCreate(&ctx->ev[0]) != cudaSuccess || cudaEventCreate(&ctx->ev[1]) != cudaSuccess ||
+        cudaEventCreate(&ctx->ev[2]) != cudaSuccess || cudaEventCreate(&ctx->ev[3]) != cudaSuccess) {
+        cudaGetLastError();
+        scc_destroy(ctx);
+        return SCC_ERR_CUDA;
+    }
+    *out = ctx;
+    return SCC_OK;
+}
+
+extern "C" int scc_destroy(scc_context *ctx)
+{
+    if (!ctx) return SCC_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    cudaFree(ctx->ws);
+    cudaFree(ctx->dFr); cudaFree(ctx->dFc); cudaFree(ctx->dBr); cudaFree(ctx->dBc); cudaFree(ctx->dlab);
+    if (ctx->hctl) cudaFreeHost(ctx->hctl);
+    for (int i = 0; i < 4; i++) if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return SCC_OK;
+}
+
+static int grid_blocks_for(scc_context *ctx, void *fn)
+{
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, GRID_THREADS, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    if (ctx->max_blocks_per_sm > 0) occ = std::min(occ, ctx->max_blocks_per_sm);
+    return occ * ctx->nsm;
+}
+
+extern "C" int scc_run(scc_context *ctx, const scc_csr_view *gv, int algo, uint32_t flags, int warp_width,
+                       uint32_t *labels_out, scc_stats *stats, void *stream_arg)
+{
+    if (!ctx || !gv) return SCC_ERR_INVALID_ARG;
+    if (stats) memset(stats, 0, sizeof(*stats));
+    const bool hong = algo == SCC_ALGO_VHONG || algo == SCC_ALGO_WHONG;
+    const bool warped = algo == SCC_ALGO_WHONG || algo == SCC_ALGO_WSLOTA;
+    if (!hong && algo != SCC_ALGO_VSLOTA && algo != SCC_ALGO_WSLOTA) return SCC_ERR_INVALID_ARG;
+    int lw = -1;
+    if (warped) {
+        switch (warp_width) {
+        case 1: lw = 0; break;
+        case 2: lw = 1; break;
+        case 4: lw = 2; break;
+        case 8: lw = 3; break;
+        case 16: lw = 4; break;
+        case 32: lw = 5; break;
+        default: return SCC_ERR_INVALID_ARG;   // the reference silently skips the BFS (scc_WCC.cu:216-246)
+        }
+    }
+    const uint32_t V = gv->num_vertices, E = gv->num_edges;
+    if (V > SCC_MAX_VERTICES || E > SCC_MAX_EDGES) return SCC_ERR_TOO_LARGE;
+    if (V == 0) return SCC_OK;
+    if (!gv->Fr || !gv->Br || (E && (!gv->Fc || !gv->Bc))) return SCC_ERR_INVALID_ARG;
+    const bool dev = (flags & SCC_FLAG_DEVICE) != 0;
+    const bool instr = (flags & SCC_FLAG_INSTRUMENT) != 0;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t st = stream_arg ? (cudaStream_t)stream_arg : ctx->stream;
+    int rc = scc_ctx_reserve(ctx, V, E);
+    if (rc != SCC_OK) return rc;
+    unsigned launches = 0;
+
+    CK(cudaEventRecord(ctx->ev[0], st));
+    Graph g{V, E, gv->Fr, gv->Fc, gv->Br, gv->Bc};
+    uint32_t *dout = labels_out;
+    if (!dev) {
+        rc = ensure_csr_mirror(ctx, V, E);
+        if (rc != SCC_OK) return rc;
+        CK(cudaMemcpyAsync(ctx->dFr, gv->Fr, ((size_t)V + 2) * 4, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ctx->dBr, gv->Br, ((size_t)V + 2) * 4, cudaMemcpyHostToDevice, st));
+        if (E) {
+            CK(cudaMemcpyAsync(ctx->dFc, gv->Fc, (size_t)E * 4, cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(ctx->dBc, gv->Bc, (size_t)E * 4, cudaMemcpyHostToDevice, st));
+        }
+        g.Fr = ctx->dFr; g.Fc = ctx->dFc; g.Br = ctx->dBr; g.Bc = ctx->dBc;
+        dout = labels_out ? ctx->dlab : nullptr;
+    }
+    if (!E) { g.Fc = g.Fc ? g.Fc : ctx->work.st; g.Bc = g.Bc ? g.Bc : ctx->work.st; }
+
+    // control block: zeroed, then the timeout
+    memset(ctx->hctl, 0, sizeof(Ctl));
+    ctx->hctl->timeout_ns = (unsigned long long)ctx->timeout_ms * 1000000ull;
+    CK(cudaMemcpyAsync(ctx->work.ctl, ctx->hctl, sizeof(Ctl), cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(ctx->work.pivkey, 0, hong ? (4 * ((size_t)V + 1) + 8) * 8 : 8, st));
+
+    const int vblocks = std::min<int>(ctx->nsm * 4, (int)((V + 255) / 256) + 1);
+    k_validate<<<vblocks, 256, 0, st>>>(g, ctx->work.ctl);
+    launches++;
+    CK(cudaGetLastError());
+
+    Params p{g, ctx->work, (flags & SCC_FLAG_TRIM1) ? 1 : 0, (flags & SCC_FLAG_TRIM2) ? 1 : 0, lw, ctx->tail_vertices};
+    bool use_block = (V <= ctx->block_max_vertices && E <= ctx->block_max_edges);
+    if (flags & SCC_FLAG_FORCE_GRID) use_block = false;
+    if (flags & SCC_FLAG_FORCE_BLOCK) use_block = true;
+    if (!ctx->coop) use_block = true;
+    int nblocks = 1;
+    CK(cudaEventRecord(ctx->ev[1], st));
+    if (use_block) {
+        void *fn = pick_block(instr, hong);
+        void *args[] = {&p};
+        CK(cudaLaunchKernel(fn, dim3(1), dim3(BLOCK_THREADS), args, 0, st));
+    } else {
+        void *fn = pick_grid(instr, hong);
+        nblocks = grid_blocks_for(ctx, fn);
+        if (nblocks <= 0) return SCC_ERR_CUDA;
+        void *args[] = {&p};
+        CK(cudaLaunchCooperativeKernel(fn, dim3(nblocks), dim3(GRID_THREADS), args, 0, st));
+    }
+    launches++;
+    CK(cudaEventRecord(ctx->ev[2], st));
+    if (dout) {
+        const int cb = std::min<int>(ctx->nsm * 8, (int)((V + 255) / 256) + 1);
+        k_canon_min<<<cb, 256, 0, st>>>(ctx->work.label, ctx->work.st, V);
+        k_canon_write<<<cb, 256, 0, st>>>(ctx->work.label, ctx->work.st, dout, V);
+        launches += 2;
+        CK(cudaGetLastError());
+        if (!dev) CK(cudaMemcpyAsync(labels_out, dout, (size_t)V * 4, cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaMemcpyAsync(ctx->hctl, ctx->work.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
+    CK(cudaEventRecord(ctx->ev[3], st));
+    CK(cudaStreamSynchronize(st));
+    const Ctl &c = *ctx->hctl;
+    if (stats) {
+        stats->num_trim1 = c.n_trim1;
+        stats->num_trim2 = c.n_trim2;
+        stats->num_pivot = c.n_pivot;
+        stats->num_sccs = c.n_trim1 + c.n_trim2 + c.n_pivot;
+        stats->edges_scanned = c.t_edges;
+        stats->vertex_visits = c.t_verts;
+        stats->passes = c.passes;
+        stats->outer_iters = c.outer;
+        stats->tail_pass = c.tail_pass;
+        stats->gpu_launches = launches;
+        stats->grid_blocks = (uint32_t)nblocks;
+        stats->used_block_path = use_block ? 1u : 0u;
+        cudaEventElapsedTime(&stats->kernel_ms, ctx->ev[1], ctx->ev[2]);
+        cudaEventElapsedTime(&stats->total_ms, ctx->ev[0], ctx->ev[3]);
+        stats->error_where = c.where;
+    }
+    if (c.error) return c.error;
+    return SCC_OK;
+}
+
+extern "C" int scc_set_tuning(scc_context *ctx, const char *key, long long value)
+{
+    if (!ctx || !key) return SCC_ERR_INVALID_ARG;
+    if (!strcmp(key, "tail_vertices")) ctx->tail_vertices = (uint32_t)value;
+    else if (!strcmp(key, "block_max_vertices")) ctx->block_max_vertices = (uint32_t)value;
+    else if (!strcmp(key, "block_max_edges")) ctx->block_max_edges = (uint32_t)value;
+    else if (!strcmp(key, "timeout_ms")) ctx->timeout_ms = (uint32_t)value;
+    else if (!strcmp(key, "max_blocks_per_sm")) ctx->max_blocks_per_sm = (int)value;
+    else return SCC_ERR_INVALID_ARG;
+    return SCC_OK;
+}

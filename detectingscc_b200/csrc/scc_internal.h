@@ -1,0 +1,38 @@
+// Host-side context of the engine (CUDA translation units only).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+
+#include "scc_device.cuh"
+
+struct scc_context {
+    int device = 0;
+    int nsm = 0;
+    int coop = 0;
+    int last_cuda_error = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    sccb::Ctl *hctl = nullptr;   // pinned copy of the control block
+
+    // device workspace (grows to the largest graph run so far)
+    char *ws = nullptr;
+    size_t ws_bytes = 0;
+    sccb::Work work{};
+
+    // device mirror of host CSR inputs
+    uint32_t *dFr = nullptr, *dFc = nullptr, *dBr = nullptr, *dBc = nullptr, *dlab = nullptr;
+    size_t capV = 0, capE = 0;
+
+    // tuning
+    uint32_t tail_vertices = 0;          // CTA 0 finishes alone below this live count
+    uint32_t block_max_vertices = 16384; // graphs up to this size run on one CTA
+    uint32_t block_max_edges = 262144;
+    uint32_t timeout_ms = 4000;          // bound on any single grid-barrier wait
+    int max_blocks_per_sm = 0;           // 0 = occupancy limit
+
+    std::mutex mu;
+};
+
+int scc_ctx_reserve(scc_context *ctx, uint32_t V, uint32_t E);

@@ -1,0 +1,707 @@
+// Phases of the four SCC drivers (vHong / wHong, scc_WCC.cu:53-998; vSlota /
+// wSlota, scc_Coloring.cu:6-701), rewritten as work-list passes over a
+// persistent launch.  Each phase cites the reference kernel whose result it
+// reproduces; the schedules differ (frontier queues instead of full-V
+// sweeps, device-side convergence instead of a host round trip per level).
+#pragma once
+#include "scc_device.cuh"
+
+namespace sccb {
+
+// A vertex list: p[0..n) or, with p == nullptr, the implicit list
+// base, base+1, ..., base+n-1.
+struct VList {
+    const uint32_t *p;
+    uint32_t n;
+    uint32_t base;
+    __device__ __forceinline__ uint32_t at(uint32_t i) const { return p ? p[i] : base + i; }
+};
+
+template <class Ex>
+__device__ __forceinline__ void count_edges(Ex &ex, unsigned warp_total)
+{
+    if constexpr (Ex::instr) {
+        if (lane_id() == 0 && warp_total) atomicAdd(&ex.ctl->t_edges, (unsigned long long)warp_total);
+    }
+}
+template <class Ex>
+__device__ __forceinline__ void count_verts(Ex &ex, bool valid)
+{
+    if constexpr (Ex::instr) {
+        unsigned m = __ballot_sync(FULL, valid);
+        if (lane_id() == 0 && m) atomicAdd(&ex.ctl->t_verts, (unsigned long long)__popc(m));
+    }
+}
+
+// Does v have a live neighbour in range r in (R, C)?  Early exit, as in
+// trim1 (scc_kernels.cu:197-222).  Self-loops count, as they do there.
+template <class Ex>
+__device__ __forceinline__ bool has_live(Ex &ex, const uint32_t *st, const uint32_t *__restrict__ R,
+                                         const uint32_t *__restrict__ C, uint32_t v, uint32_t r, uint32_t V)
+{
+    uint32_t e = __ldg(&R[v]), end = __ldg(&R[v + 1]);
+    bool found = false;
+    uint32_t e0 = e;
+    for (; e < end; e++) {
+        if ((st[guard_id(__ldg(&C[e]), V, ex.ctl)] & RMASK) == r) { found = true; e++; break; }
+    }
+    if constexpr (Ex::instr) atomicAdd(&ex.ctl->t_edges, (unsigned long long)(e - e0));
+    return found;
+}
+
+// Up to two live same-range neighbours of x in (R, C); *first gets the
+// first one (scc_kernels.cu:250-261).
+__device__ __forceinline__ uint32_t count_upto2(const uint32_t *st, const uint32_t *__restrict__ R,
+                                                const uint32_t *__restrict__ C, uint32_t x,
+                                                uint32_t r, uint32_t *first, uint32_t V, Ctl *ctl)
+{
+    uint32_t n = 0;
+    for (uint32_t e = __ldg(&R[x]), end = __ldg(&R[x + 1]); e < end; e++) {
+        uint32_t u = guard_id(__ldg(&C[e]), V, ctl);
+        if ((st[u] & RMASK) == r) {
+            n++;
+            if (n == 2u) break;
+            if (first) *first = u;
+        }
+    }
+    return n;
+}
+
+// trim2 decision for v (scc_kernels.cu:236-348): the partner k, possibly v
+// itself through a self-loop, or 0.
+__device__ __forceinline__ uint32_t trim2_partner(const Graph &g, const uint32_t *st, uint32_t v, uint32_t r, Ctl *c)
+{
+    uint32_t k = 0;
+    if (count_upto2(st, g.Br, g.Bc, v, r, &k, g.V, c) == 1u) {
+        for (uint32_t e = __ldg(&g.Fr[v]), end = __ldg(&g.Fr[v + 1]); e < end; e++) {
+            if (__ldg(&g.Fc[e]) == k) {
+                if (count_upto2(st, g.Br, g.Bc, k, r, nullptr, g.V, c) == 1u) return k;
+                break;
+            }
+        }
+    }
+    k = 0;
+    if (count_upto2(st, g.Fr, g.Fc, v, r, &k, g.V, c) == 1u) {
+        for (uint32_t e = __ldg(&g.Br[v]), end = __ldg(&g.Br[v + 1]); e < end; e++) {
+            if (__ldg(&g.Bc[e]) == k) {
+                if (count_upto2(st, g.Fr, g.Fc, k, r, nullptr, g.V, c) == 1u) return k;
+                break;
+            }
+        }
+    }
+    return 0;
+}
+
+// ---------------------------------------------------------------------
+// init: every vertex live in range 0 (the reference's cudaMemset of range
+// and tags, scc_WCC.cu:630-631); optionally fold the first-pivot key.
+// ---------------------------------------------------------------------
+template <class Ex>
+__device__ bool ph_init(Ex &ex, const Graph &g, const Work &w, bool fold_pivot)
+{
+    return run_pass(ex, [&](unsigned, unsigned) {
+        unsigned long long best = 0;
+        for (uint32_t i = ex.tid(); i <= g.V; i += ex.nthr()) {
+            w.st[i] = (i == 0u) ? DEAD : 0u;
+            w.stamp[i] = 0u;
+            if (fold_pivot && i != 0u) {
+                unsigned long long k = pivot_key(g, i);
+                best = k > best ? k : best;
+            }
+        }
+        if (fold_pivot) block_max_atomic(best, &w.pivkey[0]);
+    });
+}
+
+// ---------------------------------------------------------------------
+// trim1, one pass decided on the state before the pass (vSlota / wSlota
+// run trim1 once, scc_Coloring.cu:507-508).  Survivors fold the first-pivot
+// key on the way (pollForFirstPivot, scc_kernels.cu:643-656).
+// ---------------------------------------------------------------------
+template <class Ex>
+__device__ bool ph_trim1_once(Ex &ex, const Graph &g, const Work &w)
+{
+    bool ok = run_pass(ex, [&](unsigned, unsigned nxt) {
+        const unsigned par = ex.gl & 1u;
+        unsigned long long best = 0;
+        for (uint32_t base = ex.wid() * 32u; base < g.V; base += ex.nwarps() * 32u) {
+            uint32_t v = base + lane_id() + 1u;
+            bool valid = v <= g.V, trim = false;
+            if (valid) {
+                uint32_t s = w.st[v];
+                if (s != DEAD) {
+                    uint32_t r = s & RMASK;
+                    trim = !has_live(ex, w.st, g.Br, g.Bc, v, r, g.V) || !has_live(ex, w.st, g.Fr, g.Fc, v, r, g.V);
+                    if (!trim) {
+                        unsigned long long k = pivot_key(g, v);
+                        best = k > best ? k : best;
+                    }
+                }
+            }
+            count_verts(ex, valid);
+            warp_push(trim, v, w.Q[0][par], &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 10);
+        }
+        block_max_atomic(best, &w.pivkey[0]);
+    });
+    if (!ok) return false;
+    const uint32_t nT = last_count(ex, C_LIST);
+    return run_pass(ex, [&](unsigned, unsigned) {
+        const uint32_t *T = w.Q[0][(ex.gl & 1u) ^ 1u];
+        for (uint32_t i = ex.tid(); i < nT; i += ex.nthr()) {
+            uint32_t v = T[i];
+            w.st[v] = DEAD;
+            w.label[v] = v;
+        }
+        if (ex.leader()) ex.ctl->n_trim1 += nT;
+    });
+}
+
+// ---------------------------------------------------------------------
+// trim1 iterated to its fixpoint (vHong / wHong, scc_WCC.cu:680-687,
+// :773-780, :808-815).  Pass 0 checks src0; a trimmed vertex queues its
+// live same-range neighbours for the next pass (stamp-deduplicated), so
+// later passes only recheck vertices that lost a neighbour.
+// ---------------------------------------------------------------------
+template <class Ex>
+__device__ bool ph_trim1_fix(Ex &ex, const Graph &g, const Work &w, VList src0)
+{
+    uint32_t nq = 0;
+    bool first = true;
+    for (unsigned it = 0;; it++) {
+        if (it > g.V + 2u) { if (ex.leader()) set_error(ex.ctl, E_NOT_CONVERGED, 30); return false; }
+        bool ok = run_pass(ex, [&](unsigned, unsigned nxt) {
+            const unsigned par = ex.gl & 1u;
+            const uint32_t tag = ex.gl + 1u;
+            VList src = first ? src0 : VList{w.Q[0][par ^ 1u], nq, 0u};
+            for (uint32_t base = ex.wid() * 32u; base < src.n; base += ex.nwarps() * 32u) {
+                uint32_t i = base + lane_id();
+                bool valid = i < src.n, trim = false;
+                uint32_t v = valid ? src.at(i) : 0u, r = 0u;
+                if (valid) {
+                    uint32_t s = w.st[v];
+                    if (s != DEAD) {
+                        r = s & RMASK;
+                        trim = !has_live(ex, w.st, g.Br, g.Bc, v, r, g.V) || !has_live(ex, w.st, g.Fr, g.Fc, v, r, g.V);
+                        if (trim) { w.st[v] = DEAD; w.label[v] = v; }
+                    }
+                }
+                count_verts(ex, valid);
+                unsigned m = __ballot_sync(FULL, trim);
+                if (lane_id() == 0 && m) atomicAdd(&ex.ctl->n_trim1, (unsigned long long)__popc(m));
+                while (m) {
+                    unsigned j = __ffs(m) - 1u;
+                    m &= m - 1u;
+                    uint32_t vj = __shfl_sync(FULL, v, j), rj = __shfl_sync(FULL, r, j);
+#pragma unroll
+                    for (int dir = 0; dir < 2; dir++) {
+                        const uint32_t *R = dir ? g.Br : g.Fr;
+                        const uint32_t *C = dir ? g.Bc : g.Fc;
+                        uint32_t beg = __ldg(&R[vj]), end = __ldg(&R[vj + 1]);
+                        for (uint32_t b = beg; b < end; b += 32u) {
+                            uint32_t e = b + lane_id();
+                            bool ok2 = e < end, push = false;
+                            uint32_t u = ok2 ? guard_id(__ldg(&C[e]), g.V, ex.ctl) : 0u;
+                            if (ok2 && (w.st[u] & RMASK) == rj) push = stamp_claim(w.stamp, u, tag);
+                            warp_push(push, u, w.Q[0][par], &ex.ctl->lc[nxt][C_FQ], g.V, ex.ctl, 11);
+                        }
+                        count_edges(ex, end - beg);
+                    }
+                }
+            }
+        });
+        if (!ok) return false;
+        first = false;
+        nq = last_count(ex, C_FQ);
+        if (nq == 0u) return true;
+    }
+}
+
+// ---------------------------------------------------------------------
+// trim2 once, decided on the state before the pass (scc_WCC.cu:792-793,
+// scc_kernels.cu:236-357).  Both members are marked; the pair counts once,
+// on its smaller id.  The reference marks both members with unsynchronised
+// byte writes (scc_kernels.cu:350-354) and can lose the trim2 tag.
+// ---------------------------------------------------------------------
+template <class Ex>
+__device__ bool ph_trim2(Ex &ex, const Graph &g, const Work &w, VList src)
+{
+    bool ok = run_pass(ex, [&](unsigned, unsigned nxt) {
+        const unsigned par = ex.gl & 1u;
+        for (uint32_t base = ex.wid() * 32u; base < src.n; base += ex.nwarps() * 32u) {
+            uint32_t i = base + lane_id();
+            bool valid = i < src.n, hit = false, cnt = false;
+            uint32_t v = valid ? src.at(i) : 0u;
+            if (valid) {
+                uint32_t s = w.st[v];
+                if (s != DEAD) {
+                    uint32_t k = trim2_partner(g, w.st, v, s & RMASK, ex.ctl);
+                    if (k) {
+                        hit = true;
+                        cnt = v <= k;
+                        w.label[v] = v < k ? v : k;
+                    }
+                }
+            }
+            count_verts(ex, valid);
+            unsigned m = __ballot_sync(FULL, cnt);
+            if (lane_id() == 0 && m) atomicAdd(&ex.ctl->n_trim2, (unsigned long long)__popc(m));
+            warp_push(hit, v, w.Q[0][par], &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 12);
+        }
+    });
+    if (!ok) return false;
+    const uint32_t nT = last_count(ex, C_LIST);
+    return run_pass(ex, [&](unsigned, unsigned) {
+        const uint32_t *T = w.Q[0][(ex.gl & 1u) ^ 1u];
+        for (uint32_t i = ex.tid(); i < nT; i += ex.nthr()) w.st[T[i]] = DEAD;
+    });
+}
+
+// ---------------------------------------------------------------------
+// Frontier expansion of one direction for the lanes of a warp.  A lane with
+// act holds vertex v of range r; its neighbours that are live, in range r
+// and not yet visited in this direction are claimed with atomicOr and
+// appended to the next frontier (warp ballot compaction).  Vertices with
+// more than HEAVY_T entries are cut into CH-entry chunks for the next pass.
+// This is fwd/bwd (scc_kernels.cu:360-445) and fwd_warp/bwd_warp
+// (include/scc_kernels.h:46-105) over a queue instead of a full sweep.
+// ---------------------------------------------------------------------
+template <class Ex>
+__device__ __forceinline__ void bfs_edge_visit(Ex &ex, const Graph &g, const Work &w, int dir, bool valid,
+                                               uint32_t nbr, uint32_t r, unsigned par, unsigned nxt)
+{
+    const uint32_t bit = dir ? BVB : FVB;
+    bool claim = false;
+    if (valid) {
+        nbr = guard_id(nbr, g.V, ex.ctl);
+        uint32_t s = w.st[nbr];
+        if ((s & (RMASK | bit)) == r) claim = !(atomicOr(&w.st[nbr], bit) & bit);
+    }
+    warp_push(claim, nbr, w.Q[dir][par], &ex.ctl->lc[nxt][C_FQ + dir], g.V, ex.ctl, 13);
+}
+
+template <class Ex>
+__device__ __forceinline__ void bfs_expand_lanes(Ex &ex, const Graph &g, const Work &w, int dir, uint32_t v,
+                                                 bool act, uint32_t r, int lw, unsigned par, unsigned nxt)
+{
+    const uint32_t *R = dir ? g.Br : g.Fr;
+    const uint32_t *C = dir ? g.Bc : g.Fc;
+    uint32_t beg = 0, deg = 0;
+    if (act) { beg = __ldg(&R[v]); deg = __ldg(&R[v + 1]) - beg; }
+    bool heavy = deg > HEAVY_T;
+    uint32_t nch = heavy ? (deg + CH - 1u) / CH : 0u;
+    if (lw > 0 && (lane_id() & ((1u << lw) - 1u)) != 0u) nch = 0u;
+    warp_push_chunks(v, nch, w.H[dir][par], &ex.ctl->lc[nxt][C_FH + dir], w.hcap, ex.ctl);
+    if (heavy) deg = 0u;
+    auto fn = [&](bool valid, uint32_t nbr, uint32_t rr) { bfs_edge_visit(ex, g, w, dir, valid, nbr, rr, par, nxt); };
+    unsigned tot = (lw < 0) ? lbs_expand(beg, deg, r, C, fn) : vw_expand(beg, deg, r, (unsigned)lw, C, fn);
+    count_edges(ex, tot);
+}
+
+// One CH-entry chunk of a heavy vertex, expanded by the whole warp.
+template <class Ex, class Fn>
+__device__ __forceinline__ void chunk_expand(Ex &ex, const uint32_t *__restrict__ R, const uint32_t *__restrict__ C,
+                                             uint2 hc, uint32_t aux, Fn &&fn)
+{
+    uint32_t beg = __ldg(&R[hc.x]) + hc.y * CH;
+    uint32_t end = min(__ldg(&R[hc.x + 1]), beg + CH);
+    for (uint32_t k = lane_id(); k < CH; k += 32u) {
+        uint32_t e = beg + k;
+        bool valid = e < end;
+        uint32_t nbr = valid ? __ldg(&C[e]) : 0u;
+        fn(valid, nbr, aux);
+    }
+    count_edges(ex, end > beg ? end - beg : 0u);
+}
+
+// Seed predicates for the first BFS pass.
+struct SeedOne {      // the single first pivot
+    uint32_t p;
+    __device__ __forceinline__ bool operator()(const Work &, uint32_t v) const { return v == p; }
+};
+struct SeedPivkey {   // per-range pivots (selectPivots, scc_kernels.cu:4-19)
+    __device__ __forceinline__ bool operator()(const Work &w, uint32_t v) const
+    {
+        uint32_t s = w.st[v];
+        return s != DEAD && key_vertex(w.pivkey[s & RMASK]) == v;
+    }
+};
+struct SeedRoot {     // colouring roots (selectPivotColoring, scc_kernels.cu:567-580)
+    __device__ __forceinline__ bool operator()(const Work &w, uint32_t v) const { return w.st[v] == v; }
+};
+
+// Forward (and backward) reachability to closure.  Pass 0 walks src, tests
+// the seed predicate, flags seeds and expands them; later passes expand the
+// frontier queues and the heavy chunks.  lw < 0 selects the load-balanced
+// warp schedule, lw >= 0 the virtual-warp schedule with W = 1 << lw.
+template <class Ex, class Seed>
+__device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed seed, bool bw, int lw)
+{
+    const unsigned gsz = (lw < 0) ? 32u : (32u >> lw);
+    bool ok = run_pass(ex, [&](unsigned, unsigned nxt) {
+        const unsigned par = ex.gl & 1u;
+        const unsigned ng = (src.n + gsz - 1u) / gsz;
+        const uint32_t bits = bw ? (FVB | BVB) : FVB;
+        for (uint32_t it = ex.wid(); it < ng; it += ex.nwarps()) {
+            unsigned slot = (lw < 0) ? lane_id() : (lane_id() >> lw);
+            uint32_t i = it * gsz + slot;
+            bool valid = i < src.n;
+            uint32_t v = valid ? src.at(i) : 0u;
+            bool act = valid && seed(w, v);
+            bool lead = (lw <= 0) || ((lane_id() & ((1u << lw) - 1u)) == 0u);
+            uint32_t r = 0;
+            if (act && lead) r = atomicOr(&w.st[v], bits) & RMASK;
+            if (lw > 0) r = __shfl_sync(FULL, r, lane_id() & ~((1u << lw) - 1u));
+            unsigned m = __ballot_sync(FULL, act && lead);
+            if (lane_id() == 0 && m) atomicAdd(&ex.ctl->n_pivot, (unsigned long long)__popc(m));
+            count_verts(ex, valid && lead);
+            bfs_expand_lanes(ex, g, w, 0, v, act, r, lw, par, nxt);
+            if (bw) bfs_expand_lanes(ex, g, w, 1, v, act, r, lw, par, nxt);
+        }
+    });
+    if (!ok) return false;
+    for (unsigned lev = 1;; lev++) {
+        const uint32_t nf = last_count(ex, C_FQ), nb = last_count(ex, C_BQ);
+        const uint32_t nhf = last_count(ex, C_FH), nhb = last_count(ex, C_BH);
+        if (nf + nb + nhf + nhb == 0u) return true;
+        if (lev > g.V + 2u) { if (ex.leader()) set_error(ex.ctl, E_NOT_CONVERGED, 40); return false; }
+        ok = run_pass(ex, [&](unsigned, unsigned nxt) {
+            const unsigned par = ex.gl & 1u, cp = par ^ 1u;
+            const uint32_t ngf = (nf + gsz - 1u) / gsz, ngb = (nb + gsz - 1u) / gsz;
+            const uint32_t nitems = nhf + nhb + ngf + ngb;
+            for (uint32_t it = ex.wid(); it < nitems; it += ex.nwarps()) {
+                if (it < nhf + nhb) {
+                    int dir = it < nhf ? 0 : 1;
+                    uint2 hc = w.H[dir][cp][dir ? it - nhf : it];
+                    uint32_t r = w.st[hc.x] & RMASK;
+                    auto fn = [&](bool valid, uint32_t nbr, uint32_t rr) { bfs_edge_visit(ex, g, w, dir, valid, nbr, rr, par, nxt); };
+                    chunk_expand(ex, dir ? g.Br : g.Fr, dir ? g.Bc : g.Fc, hc, r, fn);
+                } else {
+                    uint32_t gi = it - nhf - nhb;
+                    int dir = gi < ngf ? 0 : 1;
+                    if (dir) gi -= ngf;
+                    const uint32_t n = dir ? nb : nf;
+                    unsigned slot = (lw < 0) ? lane_id() : (lane_id() >> lw);
+                    uint32_t i = gi * gsz + slot;
+                    bool valid = i < n;
+                    uint32_t v = valid ? w.Q[dir][cp][i] : 0u;
+                    uint32_t r = valid ? (w.st[v] & RMASK) : 0u;
+                    bool lead = (lw <= 0) || ((lane_id() & ((1u << lw) - 1u)) == 0u);
+                    count_verts(ex, valid && lead);
+                    bfs_expand_lanes(ex, g, w, dir, v, valid, r, lw, par, nxt);
+                }
+            }
+        });
+        if (!ok) return false;
+    }
+}
+
+// ---------------------------------------------------------------------
+// Label propagation over in-edges to a fixpoint:
+//   MAXP = true : colour = max id reachable (colorPropagation,
+//                 scc_kernels.cu:539-564, pulls the max over out-neighbours)
+//   MAXP = false: name = min id reachable (the "WCC" of propagateRange1 /
+//                 propagateRange2, scc_kernels.cu:496-536)
+// Written as a push over the reverse CSR: when w's value moves, its
+// in-neighbours are updated with atomicMax / atomicMin and queued.
+// ---------------------------------------------------------------------
+template <bool MAXP, class Ex>
+__device__ __forceinline__ void prop_visit(Ex &ex, const Graph &g, const Work &w, bool valid, uint32_t u,
+                                           uint32_t c, unsigned par, unsigned nxt, uint32_t tag)
+{
+    bool push = false;
+    if (valid) {
+        u = guard_id(u, g.V, ex.ctl);
+        uint32_t s = w.st[u];
+        if (MAXP) {
+            if (s < c) push = atomicMax(&w.st[u], c) < c && stamp_claim(w.stamp, u, tag);
+        } else {
+            if (s != DEAD && s > c) push = atomicMin(&w.st[u], c) > c && stamp_claim(w.stamp, u, tag);
+        }
+    }
+    warp_push(push, u, w.Q[0][par], &ex.ctl->lc[nxt][C_FQ], g.V, ex.ctl, 14);
+}
+
+template <bool MAXP, class Ex>
+__device__ bool ph_propagate(Ex &ex, const Graph &g, const Work &w, VList src0)
+{
+    uint32_t nq = 0, nh = 0;
+    bool first = true;
+    for (unsigned lev = 0;; lev++) {
+        if (lev > g.V + 2u) { if (ex.leader()) set_error(ex.ctl, E_NOT_CONVERGED, 50); return false; }
+        bool ok = run_pass(ex, [&](unsigned, unsigned nxt) {
+            const unsigned par = ex.gl & 1u, cp = par ^ 1u;
+            const uint32_t tag = ex.gl + 1u;
+            VList src = first ? src0 : VList{w.Q[0][cp], nq, 0u};
+            const uint32_t hn = first ? 0u : nh;
+            const uint32_t ng = (src.n + 31u) / 32u;
+            auto fn = [&](bool valid, uint32_t u, uint32_t c) { prop_visit<MAXP>(ex, g, w, valid, u, c, par, nxt, tag); };
+            for (uint32_t it = ex.wid(); it < hn + ng; it += ex.nwarps()) {
+                if (it < hn) {
+                    uint2 hc = w.H[0][cp][it];
+                    chunk_expand(ex, g.Br, g.Bc, hc, w.st[hc.x] & RMASK, fn);
+                } else {
+                    uint32_t i = (it - hn) * 32u + lane_id();
+                    bool valid = i < src.n;
+                    uint32_t v = valid ? src.at(i) : 0u;
+                    uint32_t c = valid ? (w.st[v] & RMASK) : 0u;
+                    uint32_t beg = 0, deg = 0;
+                    if (valid) { beg = __ldg(&g.Br[v]); deg = __ldg(&g.Br[v + 1]) - beg; }
+                    bool heavy = deg > HEAVY_T;
+                    warp_push_chunks(v, heavy ? (deg + CH - 1u) / CH : 0u, w.H[0][par],
+                                     &ex.ctl->lc[nxt][C_FH], w.hcap, ex.ctl);
+                    if (heavy) deg = 0u;
+                    count_verts(ex, valid);
+                    count_edges(ex, lbs_expand(beg, deg, c, g.Bc, fn));
+                }
+            }
+        });
+        if (!ok) return false;
+        first = false;
+        nq = last_count(ex, C_FQ);
+        nh = last_count(ex, C_FH);
+        if (nq + nh == 0u) return true;
+    }
+}
+
+// ---------------------------------------------------------------------
+// Hong update (scc_kernels.cu:124-142): FV and BV -> the SCC of the range's
+// pivot; otherwise the vertex moves to one of three fresh sub-range names
+// and is appended to the next live list.  With fold, the survivors also
+// bid for the pivot of their new range, which replaces the reference's
+// separate pollForPivots/selectPivots launches (scc_WCC.cu:860-862).
+// ---------------------------------------------------------------------
+template <class Ex>
+__device__ bool ph_hong_update(Ex &ex, const Graph &g, const Work &w, VList src, uint32_t *Lout,
+                               bool single, bool fold)
+{
+    return run_pass(ex, [&](unsigned, unsigned nxt) {
+        for (uint32_t base = ex.wid() * 32u; base < src.n; base += ex.nwarps() * 32u) {
+            uint32_t i = base + lane_id();
+            bool valid = i < src.n, surv = false;
+            uint32_t v = valid ? src.at(i) : 0u, nr = 0u;
+            if (valid) {
+                uint32_t s = w.st[v];
+                if (s != DEAD) {
+                    uint32_t p = key_vertex(w.pivkey[single ? 0u : (s & RMASK)]);
+                    if ((s & FVB) && (s & BVB)) {
+                        w.st[v] = DEAD;
+                        w.label[v] = p;
+                    } else {
+                        nr = split_name(g.V, p, s);
+                        w.st[v] = nr;
+                        surv = true;
+                    }
+                }
+            }
+            count_verts(ex, valid);
+            warp_push(surv, v, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 15);
+            if (fold) range_max_atomic(surv, nr, surv ? pivot_key(g, v) : 0ull, w.pivkey);
+        }
+    });
+}
+
+// Slota: the first FW-BW's SCC is final; every other live vertex starts
+// the colouring with colour = its own id (assignUniqueRange,
+// scc_kernels.cu:477-484) and is appended to the live list.
+template <class Ex>
+__device__ bool ph_slota_first_update(Ex &ex, const Graph &g, const Work &w, uint32_t *Lout)
+{
+    return run_pass(ex, [&](unsigned, unsigned nxt) {
+        const uint32_t p = key_vertex(w.pivkey[0]);
+        for (uint32_t base = ex.wid() * 32u; base < g.V; base += ex.nwarps() * 32u) {
+            uint32_t v = base + lane_id() + 1u;
+            bool valid = v <= g.V, surv = false;
+            if (valid) {
+                uint32_t s = w.st[v];
+                if (s != DEAD) {
+                    if ((s & FVB) && (s & BVB)) { w.st[v] = DEAD; w.label[v] = p; }
+                    else { w.st[v] = v; surv = true; }
+                }
+            }
+            count_verts(ex, valid);
+            warp_push(surv, v, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 16);
+        }
+    });
+}
+
+// Slota peel end (updateColoring, scc_kernels.cu:614-623; fwdColoring's
+// rangeSet, :607): visited vertices belong to their root's SCC; the rest
+// restart from their own colour and form the next live list.
+template <class Ex>
+__device__ bool ph_slota_peel_update(Ex &ex, const Graph &g, const Work &w, VList src, uint32_t *Lout)
+{
+    return run_pass(ex, [&](unsigned, unsigned nxt) {
+        for (uint32_t base = ex.wid() * 32u; base < src.n; base += ex.nwarps() * 32u) {
+            uint32_t i = base + lane_id();
+            bool valid = i < src.n, surv = false;
+            uint32_t v = valid ? src.at(i) : 0u;
+            if (valid) {
+                uint32_t s = w.st[v];
+                if (s & FVB) { w.st[v] = DEAD; w.label[v] = s & RMASK; }
+                else { w.st[v] = v; surv = true; }
+            }
+            count_verts(ex, valid);
+            warp_push(surv, v, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 17);
+        }
+    });
+}
+
+// Hong: compact the live list and give every live vertex its own id as
+// name (assignUniqueRange, scc_kernels.cu:477-484) before the min-label
+// propagation.
+template <class Ex>
+__device__ bool ph_compact_rename(Ex &ex, const Graph &g, const Work &w, VList src, uint32_t *Lout)
+{
+    return run_pass(ex, [&](unsigned, unsigned nxt) {
+        for (uint32_t base = ex.wid() * 32u; base < src.n; base += ex.nwarps() * 32u) {
+            uint32_t i = base + lane_id();
+            bool valid = i < src.n, surv = false;
+            uint32_t v = valid ? src.at(i) : 0u;
+            if (valid && w.st[v] != DEAD) { w.st[v] = v; surv = true; }
+            count_verts(ex, valid);
+            warp_push(surv, v, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 18);
+        }
+    });
+}
+
+// Per-range pivot bids over a list (pollForPivots, scc_kernels.cu:57-74).
+template <class Ex>
+__device__ bool ph_pivots(Ex &ex, const Graph &g, const Work &w, VList src)
+{
+    return run_pass(ex, [&](unsigned, unsigned) {
+        for (uint32_t base = ex.wid() * 32u; base < src.n; base += ex.nwarps() * 32u) {
+            uint32_t i = base + lane_id();
+            bool valid = i < src.n;
+            uint32_t v = valid ? src.at(i) : 0u;
+            uint32_t r = valid ? (w.st[v] & RMASK) : 0u;
+            range_max_atomic(valid, r, valid ? pivot_key(g, v) : 0ull, w.pivkey);
+        }
+    });
+}
+
+// ---------------------------------------------------------------------
+// drivers
+// ---------------------------------------------------------------------
+struct Carry {
+    unsigned gl;
+    unsigned lsel;
+    uint32_t nL;
+};
+
+enum { RUN_DONE = 0, RUN_SWITCH = 1, RUN_ERROR = -1 };
+
+// Hong main loop (scc_WCC.cu:851-930): per-range pivots, FW-BW, update,
+// until no vertex is left.  Entry: live list L[lsel] with nL entries and
+// the pivot bids of their ranges already in pivkey.
+template <class Ex>
+__device__ int hong_loop(Ex &ex, const Graph &g, const Work &w, Carry &cy, uint32_t tail_n)
+{
+    while (cy.nL > 0u) {
+        if (Ex::grid && cy.nL <= tail_n) { cy.gl = ex.gl; return RUN_SWITCH; }
+        if (ex.leader()) ex.ctl->outer++;
+        const VList L{w.L[cy.lsel], cy.nL, 0u};
+        if (!ph_bfs(ex, g, w, L, SeedPivkey{}, true, -1)) return RUN_ERROR;
+        if (!ph_hong_update(ex, g, w, L, w.L[cy.lsel ^ 1u], false, true)) return RUN_ERROR;
+        cy.nL = last_count(ex, C_LIST);
+        cy.lsel ^= 1u;
+        cy.gl = ex.gl;
+    }
+    return RUN_DONE;
+}
+
+// First pivot over the live vertices after trim1 to fixpoint
+// (pollForFirstPivot / selectFirstPivot, scc_WCC.cu:701-703).
+template <class Ex>
+__device__ bool ph_first_pivot(Ex &ex, const Graph &g, const Work &w)
+{
+    return run_pass(ex, [&](unsigned, unsigned) {
+        unsigned long long best = 0;
+        for (uint32_t v = ex.tid() + 1u; v <= g.V; v += ex.nthr()) {
+            if (w.st[v] != DEAD) {
+                unsigned long long k = pivot_key(g, v);
+                best = k > best ? k : best;
+            }
+        }
+        block_max_atomic(best, &w.pivkey[0]);
+    });
+}
+
+__device__ __forceinline__ unsigned long long vld64(const unsigned long long *p)
+{
+    return *(const volatile unsigned long long *)p;
+}
+
+// The first FW-BW of every driver, from the single pivot in pivkey[0]
+// (scc_WCC.cu:717-743, scc_Coloring.cu:539-565; wHong / wSlota run it with
+// the virtual-warp schedule, scc_WCC.cu:209-317, scc_Coloring.cu:154-263).
+template <class Ex>
+__device__ bool first_fwbw(Ex &ex, const Graph &g, const Work &w, int lw)
+{
+    const unsigned long long k = vld64(&w.pivkey[0]);
+    const uint32_t p = k ? key_vertex(k) : 0u;
+    return ph_bfs(ex, g, w, VList{nullptr, k ? 1u : 0u, p}, SeedOne{p}, true, lw);
+}
+
+// vHong / wHong up to the main loop (scc_WCC.cu:573-848): trim1*, first
+// pivot, FW-BW, update, trim1*, trim2, trim1*, "WCC", first per-range pivots.
+template <class Ex>
+__device__ int hong_front(Ex &ex, const Graph &g, const Work &w, bool t1, bool t2, int lw, Carry &cy)
+{
+    const VList all{nullptr, g.V, 1u};
+    if (!ph_init(ex, g, w, !t1)) return RUN_ERROR;
+    if (t1) {
+        if (!ph_trim1_fix(ex, g, w, all)) return RUN_ERROR;
+        if (!ph_first_pivot(ex, g, w)) return RUN_ERROR;
+    }
+    if (!first_fwbw(ex, g, w, lw)) return RUN_ERROR;
+    if (!ph_hong_update(ex, g, w, all, w.L[0], true, false)) return RUN_ERROR;
+    uint32_t n0 = last_count(ex, C_LIST);
+    if (t1 && !ph_trim1_fix(ex, g, w, VList{w.L[0], n0, 0u})) return RUN_ERROR;
+    if (t2 && !ph_trim2(ex, g, w, VList{w.L[0], n0, 0u})) return RUN_ERROR;
+    if (t1 && t2 && !ph_trim1_fix(ex, g, w, VList{w.L[0], n0, 0u})) return RUN_ERROR;
+    if (!ph_compact_rename(ex, g, w, VList{w.L[0], n0, 0u}, w.L[1])) return RUN_ERROR;
+    cy.lsel = 1u;
+    cy.nL = last_count(ex, C_LIST);
+    const VList L{w.L[1], cy.nL, 0u};
+    if (!ph_propagate<false>(ex, g, w, L)) return RUN_ERROR;
+    if (!ph_pivots(ex, g, w, L)) return RUN_ERROR;
+    cy.gl = ex.gl;
+    return RUN_DONE;
+}
+
+// vSlota / wSlota up to the colouring loop (scc_Coloring.cu:403-587):
+// trim1 once, first pivot, FW-BW, update.  t2 is not used by the
+// reference's Slota drivers.
+template <class Ex>
+__device__ int slota_front(Ex &ex, const Graph &g, const Work &w, bool t1, int lw, Carry &cy)
+{
+    if (!ph_init(ex, g, w, !t1)) return RUN_ERROR;
+    if (t1 && !ph_trim1_once(ex, g, w)) return RUN_ERROR;
+    if (!first_fwbw(ex, g, w, lw)) return RUN_ERROR;
+    if (!ph_slota_first_update(ex, g, w, w.L[0])) return RUN_ERROR;
+    cy.lsel = 0u;
+    cy.nL = last_count(ex, C_LIST);
+    cy.gl = ex.gl;
+    return RUN_DONE;
+}
+
+// Colouring peels (scc_Coloring.cu:590-637): max-colour propagation, roots
+// colour == id, forward reachability inside the colour, update.
+template <class Ex>
+__device__ int slota_peels(Ex &ex, const Graph &g, const Work &w, Carry &cy, uint32_t tail_n)
+{
+    while (cy.nL > 0u) {
+        if (Ex::grid && cy.nL <= tail_n) { cy.gl = ex.gl; return RUN_SWITCH; }
+        if (ex.leader()) ex.ctl->outer++;
+        const VList L{w.L[cy.lsel], cy.nL, 0u};
+        if (!ph_propagate<true>(ex, g, w, L)) return RUN_ERROR;
+        if (!ph_bfs(ex, g, w, L, SeedRoot{}, false, -1)) return RUN_ERROR;
+        if (!ph_slota_peel_update(ex, g, w, L, w.L[cy.lsel ^ 1u])) return RUN_ERROR;
+        cy.nL = last_count(ex, C_LIST);
+        cy.lsel ^= 1u;
+        cy.gl = ex.gl;
+    }
+    return RUN_DONE;
+}
+
+}  // namespace sccb

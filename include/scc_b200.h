@@ -1,0 +1,176 @@
+/*
+ * scc_b200.h -- C ABI of the B200 SCC engine (libscc_b200.so).
+ *
+ * Plain C types only: pointers, sizes, integer codes.  No function crosses
+ * the ABI with an exception or a process exit; every entry point returns an
+ * scc_status code.
+ *
+ * Graph layout is the reference's (load.cpp:49-113): vertices are 1..V;
+ * Fr and Br hold V+2 offsets with Fr[0] = Fr[1] = 0 and Fr[V+1] = E; vertex v
+ * owns Fc[Fr[v] .. Fr[v+1]); (Br, Bc) is the transpose.  RSize in the
+ * reference's signatures is V and CSize is E (load.cpp:133-134).
+ */
+#ifndef SCC_B200_H
+#define SCC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+typedef enum {
+    SCC_OK = 0,
+    SCC_ERR_INVALID_ARG = 1,    /* bad algorithm, warp width, null pointer */
+    SCC_ERR_CUDA = 2,           /* a CUDA runtime call failed */
+    SCC_ERR_OOM = 3,            /* device allocation failed */
+    SCC_ERR_TOO_LARGE = 4,      /* V or E above SCC_MAX_VERTICES / SCC_MAX_EDGES */
+    SCC_ERR_NO_DEVICE = 5,      /* no CUDA device / wrong architecture */
+    SCC_ERR_BUDGET = 6,         /* batch or serving memory budget exceeded */
+    SCC_ERR_IO = 7,             /* graph file could not be read */
+    SCC_ERR_OVERFLOW = 20,      /* an internal work list overflowed (bug guard) */
+    SCC_ERR_NOT_CONVERGED = 21, /* a convergence loop hit its iteration cap */
+    SCC_ERR_TIMEOUT = 22,       /* a grid barrier wait timed out */
+    SCC_ERR_BAD_GRAPH = 23      /* offsets not monotone / ids outside [1, V] */
+} scc_status;
+
+/* ---- algorithms: the reference's -a letters (scc.cu:78-102) ------------- */
+typedef enum {
+    SCC_ALGO_VHONG = 'g',  /* vHong  scc_WCC.cu:573       */
+    SCC_ALGO_VSLOTA = 'h', /* vSlota scc_Coloring.cu:403  */
+    SCC_ALGO_WHONG = 'x',  /* wHong  scc_WCC.cu:53        */
+    SCC_ALGO_WSLOTA = 'y'  /* wSlota scc_Coloring.cu:6    */
+} scc_algo;
+
+/* ---- flags ------------------------------------------------------------- */
+#define SCC_FLAG_TRIM1 0x1u          /* -p 1 */
+#define SCC_FLAG_TRIM2 0x2u          /* -q 1 (used by Hong; Slota ignores it, as the reference does) */
+#define SCC_FLAG_DEVICE 0x4u         /* CSR arrays and labels_out are device pointers */
+#define SCC_FLAG_INSTRUMENT 0x8u     /* count adjacency entries / vertex visits (slower) */
+#define SCC_FLAG_FORCE_GRID 0x10u    /* always use the whole-GPU persistent launch */
+#define SCC_FLAG_FORCE_BLOCK 0x20u   /* always use the single-CTA launch */
+
+#define SCC_MAX_VERTICES 268435454u  /* 2^28 - 2 */
+#define SCC_MAX_EDGES 4294967040u     /* 2^32 - 256 */
+
+typedef struct {
+    uint32_t num_vertices;  /* V  (RSize) */
+    uint32_t num_edges;     /* E  (CSize) */
+    const uint32_t *Fr;     /* V+2 forward offsets  */
+    const uint32_t *Fc;     /* E forward columns    */
+    const uint32_t *Br;     /* V+2 reverse offsets  */
+    const uint32_t *Bc;     /* E reverse columns    */
+} scc_csr_view;
+
+typedef struct {
+    uint64_t num_sccs;       /* trim1 + trim2 + pivot SCCs: the reference's "Number Of Sccs" */
+    uint64_t num_trim1;      /* the reference's numberOf1Sccs (scc_WCC.cu:948) */
+    uint64_t num_trim2;      /* trim-2 pairs */
+    uint64_t num_pivot;      /* SCCs found from a pivot / colouring root */
+    uint64_t edges_scanned;  /* adjacency entries read (SCC_FLAG_INSTRUMENT) */
+    uint64_t vertex_visits;  /* vertex visits (SCC_FLAG_INSTRUMENT) */
+    uint32_t passes;         /* device passes (barrier-separated steps) */
+    uint32_t outer_iters;    /* Hong main-loop iterations / Slota colouring peels */
+    uint32_t tail_pass;      /* pass at which one CTA took over (0 = never) */
+    uint32_t gpu_launches;   /* kernels this call launched */
+    uint32_t grid_blocks;    /* CTAs of the main launch */
+    uint32_t used_block_path;/* 1 when the single-CTA launch ran the graph */
+    float kernel_ms;         /* main SCC kernel, CUDA events on the call's stream */
+    float total_ms;          /* whole call on the device, copies included */
+    int32_t error_where;     /* internal location of a device-side error */
+} scc_stats;
+
+typedef struct scc_context scc_context;
+
+/* Create a context on CUDA device `device` (owns a stream and a device
+ * workspace that grows to the largest graph it has run). */
+int scc_create(int device, scc_context **out);
+int scc_destroy(scc_context *ctx);
+
+/* Run one SCC decomposition.
+ *   algo        one of scc_algo ('g', 'h', 'x', 'y')
+ *   flags       SCC_FLAG_*
+ *   warp_width  virtual-warp width W for 'x' / 'y' (1, 2, 4, 8, 16, 32);
+ *               ignored for 'g' / 'h'
+ *   labels_out  V entries or NULL: labels_out[i] = smallest vertex id of
+ *               the SCC of vertex i+1 (1-based ids, canonical labels)
+ *   stats       optional
+ *   stream      cudaStream_t to run on, or NULL for the context's stream
+ * With SCC_FLAG_DEVICE the CSR arrays and labels_out are device pointers;
+ * otherwise they are host pointers and the call copies them.  Synchronous:
+ * returns after the result (and the labels) are complete.
+ * Replaces the bodies of vHong / vSlota / wHong / wSlota (scc.h:49-52,
+ * scc_WCC.cu:53,573, scc_Coloring.cu:6,403), which return nothing and
+ * print their count. */
+int scc_run(scc_context *ctx, const scc_csr_view *g, int algo, uint32_t flags, int warp_width,
+            uint32_t *labels_out, scc_stats *stats, void *stream);
+
+/* Tuning knobs (used by tests and the batch autotuner):
+ *   "tail_vertices"       live-vertex count under which CTA 0 finishes alone
+ *   "block_max_vertices"  graphs up to this V run on the single-CTA path
+ *   "block_max_edges"     ... and up to this E
+ *   "timeout_ms"          bound on any grid-barrier wait (default 4000)
+ *   "max_blocks_per_sm"   cap on CTAs per SM of the persistent launch */
+int scc_set_tuning(scc_context *ctx, const char *key, long long value);
+
+/* Human-readable text for a status code. */
+const char *scc_status_string(int status);
+
+/* Library version string. */
+const char *scc_version(void);
+
+/* ---- graph files ------------------------------------------------------ */
+/* A host CSR owned by the library (arrays allocated with new[], as the
+ * reference loader does, load.cpp:52-115). */
+typedef struct {
+    uint32_t V, E;
+    uint32_t *Fr, *Fc, *Br, *Bc;
+    uint32_t *Pr;           /* METIS partition ids, zero-filled (detectSCC only) */
+} scc_host_graph;
+
+/* Read a GTgraph text file (load.cpp:12-140 semantics) or a binary CSR file
+ * ("SCCBIN01", u64 V, u64 E, Fr[V+2], Fc[E], Br[V+2], Bc[E], uint32 LE). */
+int scc_load_graph(const char *path, scc_host_graph *out);
+/* Write the binary CSR format. */
+int scc_save_binary(const char *path, const scc_host_graph *g);
+/* Build forward + reverse CSR from E arcs (1-based ids in [1, V]). */
+int scc_graph_from_arcs(uint32_t V, uint64_t E, const uint32_t *src, const uint32_t *dst,
+                        scc_host_graph *out);
+void scc_free_host_graph(scc_host_graph *g);
+
+/* ---- reference-compatible driver call ----------------------------------- */
+/* Runs one of the reference drivers with its exact stdout: for 'g' the line
+ * "numberOf1Sccs: N\n", then "\nNumber Of Sccs : N" and "\nTime : T" (ms,
+ * from entry to the count, scc_WCC.cu:577-581,948-967).  Returns a status
+ * instead of exiting.  The C++ shims vHong / vSlota / wHong / wSlota
+ * (include/scc_compat.h) call it. */
+int scc_reference_call(int algo, uint32_t CSize, uint32_t RSize, const uint32_t *Fc, const uint32_t *Fr,
+                       const uint32_t *Bc, const uint32_t *Br, int t1, int t2, int warp_width,
+                       uint64_t *num_sccs_out);
+
+/* ---- batched form: many independent graphs, one persistent launch ------ */
+typedef struct scc_batch scc_batch;
+
+/* Upload `n` graphs (host CSR views) into one device arena.  The graphs stay
+ * resident until scc_batch_destroy. */
+int scc_batch_create(scc_context *ctx, const scc_csr_view *graphs, uint32_t n, scc_batch **out);
+/* Run all graphs of the batch; labels_out (host) receives the concatenation
+ * of every graph's V labels in batch order, counts_out (host, optional)
+ * n entries of scc_batch_result. */
+typedef struct {
+    uint64_t num_sccs;
+    uint64_t num_trim1;
+    int32_t status;
+    uint32_t reserved;
+} scc_batch_result;
+int scc_batch_run(scc_batch *b, int algo, uint32_t flags, int warp_width, uint32_t *labels_out,
+                  scc_batch_result *results, scc_stats *stats);
+int scc_batch_destroy(scc_batch *b);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SCC_B200_H */

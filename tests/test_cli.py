@@ -1,0 +1,41 @@
+"""The drop-in ./scc command line: argument handling (no GPU needed)."""
+import subprocess
+
+import pytest
+
+HELP = (
+    "To execute:\n"
+    "./scc -a [g/h/x/y/d] -p [0/1] -q [0/1] -w [1/2/4/8/16/32] -f <file>\n"
+    "-a algorith to use   g - vHong, h - vSlota, x - wHong, y - wSlota, d - detectSCC\n"
+    "-p Trim-1 enable\n-q Trim-2 enable\n-w warp size\n-f input file\n"
+    "Please note that the input graph must be in GTgraph format\n"
+    "If not provided the results are undefined\n")
+
+
+def _run(native, *args):
+    return subprocess.run([native.CLI_PATH, *args], capture_output=True, text=True, timeout=60)
+
+
+def test_too_few_arguments_prints_help(native):
+    r = _run(native, "-a", "g")
+    assert r.returncode == 1 and r.stdout == HELP
+
+
+def test_detect_scc_is_not_provided(native, tmp_path):
+    r = _run(native, "-a", "d", "-p", "1", "-q", "1", "-w", "1", "-f", str(tmp_path / "x.gr"))
+    assert r.returncode == 1 and "detectSCC" in r.stderr
+
+
+def test_bad_warp_width_rejected(native, tmp_path):
+    r = _run(native, "-a", "y", "-p", "1", "-q", "1", "-w", "3", "-f", str(tmp_path / "x.gr"))
+    assert r.returncode == 1
+
+
+def test_unknown_algorithm_prints_help(native, tmp_path):
+    r = _run(native, "-a", "z", "-p", "1", "-q", "1", "-w", "1", "-f", str(tmp_path / "x.gr"))
+    assert r.returncode == 1 and r.stdout == HELP
+
+
+def test_unreadable_graph(native, tmp_path):
+    r = _run(native, "-a", "g", "-p", "1", "-q", "1", "-w", "1", "-f", str(tmp_path / "missing.gr"))
+    assert r.returncode == 1 and r.stdout.startswith("Error Reading graph file")
