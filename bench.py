@@ -1,0 +1,350 @@
+"""Benchmark of the SCC hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config cfg2|cfg1|cfg3] [--scale S]
+
+Default workload (the configuration the headline metric is quoted on):
+vSlota with trim-1 and trim-2 flags (-a h -p 1 -q 1) on a seeded synthetic
+R-MAT graph, scale 22 (4,194,304 vertices), edge factor 16,
+(a, b, c, d) = (0.57, 0.19, 0.19, 0.05), self-loops and duplicates removed.
+No public dataset is used.
+
+One step = one complete SCC decomposition of the graph (every phase of the
+driver, labels canonicalised and written).
+  value : Medges/s with the CSR already resident in HBM (device pointers),
+          L2 flushed (256 MiB write) before every step, CUDA events on the
+          launching stream, max over ranks.
+  e2e   : the same call through the C ABI with HOST (pinned) CSR buffers:
+          the H2D copy of the CSR and the D2H copy of the labels are inside
+          the timed region.
+With --gpus N > 1 (torchrun) every rank runs an independent replica of the
+graph (the plain path does not shard); value = N * E / max-over-ranks time.
+
+--impl reference times the reference's CPU-side answer for this path on the
+host cores: the reference has no CPU SCC implementation, so this is the
+project's iterative Tarjan oracle (one core, a full decomposition per step).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    "cfg1": dict(algo="g", t1=True, t2=False, warp=1,
+                 desc="vHong -p 1 -q 0 on 1,024 vertices + 8,192 uniform arcs + 16 planted cycles (len 4-32)"),
+    "cfg2": dict(algo="h", t1=True, t2=True, warp=1,
+                 desc="vSlota -p 1 -q 1 on R-MAT scale 22, edge factor 16, (0.57,0.19,0.19,0.05), "
+                      "self-loops and duplicates removed"),
+    "cfg3": dict(algo="y", t1=True, t2=True, warp=8,
+                 desc="wSlota -w 8 -p 1 -q 1 on a 4096x4096 grid, 70% bidirectional pairs, 30% one "
+                      "random orientation, +0.1% uniform long-range arcs"),
+}
+
+
+def _gen_graph(cfg: str, scale: int | None, device):
+    from detectingscc_b200 import graphs
+    if cfg == "cfg1":
+        return graphs.planted_random(seed=1, device=device)
+    if cfg == "cfg2":
+        return graphs.rmat(scale or 22, seed=1, device=device)
+    if cfg == "cfg3":
+        return graphs.grid(scale or 4096, seed=1, device=device)
+    raise ValueError(cfg)
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _traffic(cfg: str):
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            t = json.load(f).get(cfg)
+        return t
+    except Exception:
+        return None
+
+
+def _dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def _max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(world: int):
+    import torch
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def run_ours(args):
+    import torch
+
+    import detectingscc_b200 as scc
+    from detectingscc_b200 import graphs
+    world, rank, local = _dist_init()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    cfg = CONFIGS[args.config]
+
+    V, s, d = _gen_graph(args.config, args.scale, dev)
+    Fr, Fc, Br, Bc = graphs.csr_from_arcs_torch(V, s, d)
+    del s, d
+    E = int(Fc.shape[0])
+    labels = torch.empty(V, dtype=torch.int32, device=dev)
+    # pinned host copies for the end-to-end leg
+    hFr, hFc, hBr, hBc = (t.cpu().pin_memory() for t in (Fr, Fc, Br, Bc))
+    hlab = torch.empty(V, dtype=torch.int32).pin_memory()
+    hg = scc.Graph(V, E, hFr.numpy().view(np.uint32), hFc.numpy().view(np.uint32), hBr.numpy().view(np.uint32),
+                   hBc.numpy().view(np.uint32))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device=dev)
+
+    eng = scc.Engine(local)
+    stream = torch.cuda.current_stream(dev)
+    sh = stream.cuda_stream
+
+    def step_dev(instrument=False):
+        return eng.run_device(V, E, Fr, Fc, Br, Bc, labels_out=labels, algo=cfg["algo"], t1=cfg["t1"],
+                              t2=cfg["t2"], warp=cfg["warp"], stream=sh, instrument=instrument)
+
+    # warm-up
+    for _ in range(args.warmup):
+        step_dev()
+    # work counters for the roofline (separate, instrumented, untimed run)
+    ins = step_dev(instrument=True).stats
+
+    clocks = ClockSampler(local)
+    _barrier(world)
+    clocks.start()
+    step_ms, kern_ms, launches = [], [], 0
+    res = None
+    for _ in range(args.steps):
+        flush.zero_()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        res = step_dev()
+        ev1.record(stream)
+        ev1.synchronize()
+        step_ms.append(ev0.elapsed_time(ev1))
+        kern_ms.append(res.stats["kernel_ms"])
+        launches += res.stats["gpu_launches"]
+    _barrier(world)
+    clk = clocks.stop()
+    t_step = _max_over_ranks(sum(step_ms) / len(step_ms), world)
+    t_kern = _max_over_ranks(sum(kern_ms) / len(kern_ms), world)
+
+    # end-to-end: host pinned CSR in, labels out, through the C ABI
+    for _ in range(max(1, args.warmup)):
+        eng.run(hg, algo=cfg["algo"], t1=cfg["t1"], t2=cfg["t2"], warp=cfg["warp"])
+    _barrier(world)
+    e2e_ms = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        r = eng.run(hg, algo=cfg["algo"], t1=cfg["t1"], t2=cfg["t2"], warp=cfg["warp"])
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    _barrier(world)
+    t_e2e = _max_over_ranks(sum(e2e_ms) / len(e2e_ms), world)
+    assert r.num_sccs == res.num_sccs
+
+    B_alg = 8 * ins["edges_scanned"] + 12 * ins["vertex_visits"]
+    peak, peak_kind = _peak_hbm()
+    achieved = B_alg / (t_kern * 1e-3) / 1e9
+    tr = _traffic(args.config if args.scale is None else None)
+    out = {
+        "metric": f"SCC Medges/s ({'vSlota' if cfg['algo'] == 'h' else cfg['algo']}, {args.config})",
+        "value": round(world * E / (t_step * 1e-3) / 1e6, 2),
+        "unit": "Medges/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(t_step, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u32",
+        "data": "synthetic (seeded generator, no dataset)",
+        "config": {"workload": f"{args.config}: {cfg['desc']}" + (f" [scale override {args.scale}]" if args.scale else ""),
+                   "V": V, "E": E, "seed": 1, "algo": cfg["algo"], "t1": cfg["t1"], "t2": cfg["t2"],
+                   "warp": cfg["warp"], "l2": "flushed before every step (256 MiB write)",
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "num_sccs": int(res.num_sccs),
+        "counts": {"trim1": int(res.num_trim1), "trim2": int(res.num_trim2), "pivot": int(res.num_pivot)},
+        "passes": res.stats["passes"], "outer_iters": res.stats["outer_iters"],
+        "kernel_ms": round(t_kern, 4),
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                     "traffic": tr.get("dram_bytes_per_launch") if tr else None,
+                     "B_alg": int(B_alg), "T_e": int(ins["edges_scanned"]), "T_v": int(ins["vertex_visits"]),
+                     "T_e_over_E": round(ins["edges_scanned"] / max(E, 1), 3),
+                     "T_v_over_V": round(ins["vertex_visits"] / max(V, 1), 3),
+                     "B_floor_GBps": round((8 * E + 12 * V) / (t_kern * 1e-3) / 1e9, 1),
+                     "kernel": "k_scc_grid (persistent cooperative SCC kernel)"},
+        "e2e": {"value": round(world * E / (t_e2e * 1e-3) / 1e6, 2), "unit": "Medges/s",
+                "ms_per_step": round(t_e2e, 3),
+                "h2d_bytes_per_step": int(4 * (2 * (V + 2) + 2 * E)),
+                "d2h_bytes_per_step": int(4 * V + 512)},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle
+        hFr_np, hFc_np = hg.Fr, hg.Fc
+        t_cpu, reps = oracle.time_tarjan(V, hFr_np, hFc_np, budget_s=20.0, max_reps=3)
+        out["cpu_baseline"] = {"value": round(E / t_cpu / 1e6, 2), "unit": "Medges/s", "cores": 1,
+                               "kind": "port", "sample": f"full graph, iterative Tarjan, median of {reps} run(s), "
+                                                         f"{t_cpu:.2f} s per run"}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    eng.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    world, rank, local = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), \
+        int(os.environ.get("LOCAL_RANK", "0"))
+    if rank != 0:
+        return
+    import torch
+
+    from detectingscc_b200 import graphs
+    from oracle import oracle
+    cfg = CONFIGS[args.config]
+    dev = torch.device("cuda", local) if torch.cuda.is_available() else torch.device("cpu")
+    V, s, d = _gen_graph(args.config, args.scale, dev)
+    Fr, Fc, Br, Bc = (t.cpu().numpy().view(np.uint32) for t in graphs.csr_from_arcs_torch(V, s, d))
+    E = int(Fc.shape[0])
+    for _ in range(args.warmup):
+        oracle.tarjan(V, Fr, Fc)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        oracle.tarjan(V, Fr, Fc)
+        times.append(time.perf_counter() - t0)
+    t = sum(times) / len(times)
+    v = round(E / t / 1e6, 2)
+    out = {
+        "impl": "reference",
+        "metric": f"SCC Medges/s ({'vSlota' if cfg['algo'] == 'h' else cfg['algo']}, {args.config})",
+        "value": v, "unit": "Medges/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(t * 1e3, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32", "data": "synthetic (seeded generator, no dataset)",
+        "config": {"workload": f"{args.config}: {cfg['desc']}", "V": V, "E": E, "seed": 1},
+        "cpu_baseline": {"value": v, "unit": "Medges/s", "cores": 1, "kind": "port",
+                         "sample": "full graph per step; the reference has no CPU SCC path, so this is the "
+                                   "project's iterative Tarjan oracle on one host core"},
+        "e2e": {"value": v, "unit": "Medges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="cfg2", choices=sorted(CONFIGS))
+    ap.add_argument("--scale", type=int, default=None, help="smaller graph (profiling aid, not a bench value)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -79,13 +79,16 @@ def test_generated_graphs_grid_path(engine, oracle_lib, gen):
 
 def test_tail_switch_to_one_cta(engine, oracle_lib):
     from detectingscc_b200 import graphs
-    V, s, d = graphs.rmat(13, seed=11)
-    g = graphs.to_graph(V, s, d)
     try:
         engine.set_tuning("tail_vertices", 1 << 30)
-        for algo in ("g", "h"):
-            res = _check(engine, oracle_lib, g, algo, 1, 1, 1, force="grid")
-            assert res.stats["tail_pass"] > 0
+        for gen in (lambda: graphs.rmat(13, seed=11), lambda: graphs.grid(64, seed=3)):
+            V, s, d = gen()
+            g = graphs.to_graph(V, s, d)
+            for algo in ("g", "h"):
+                for t1, t2 in ((1, 1), (0, 0)):
+                    res = _check(engine, oracle_lib, g, algo, 1, t1, t2, force="grid")
+                    # CTA 0 takes over at the first main-loop iteration / peel
+                    assert res.stats["outer_iters"] == 0 or res.stats["tail_pass"] > 0
     finally:
         engine.set_tuning("tail_vertices", 0)
 
