@@ -223,13 +223,14 @@ def run_ours(args):
     t_kern = _max_over_ranks(sum(kern_ms) / len(kern_ms), world)
 
     # end-to-end: host pinned CSR in, labels out, through the C ABI
+    hlab_np = hlab.numpy().view(np.uint32)
     for _ in range(max(1, args.warmup)):
-        eng.run(hg, algo=cfg["algo"], t1=cfg["t1"], t2=cfg["t2"], warp=cfg["warp"])
+        eng.run(hg, algo=cfg["algo"], t1=cfg["t1"], t2=cfg["t2"], warp=cfg["warp"], out=hlab_np)
     _barrier(world)
     e2e_ms = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        r = eng.run(hg, algo=cfg["algo"], t1=cfg["t1"], t2=cfg["t2"], warp=cfg["warp"])
+        r = eng.run(hg, algo=cfg["algo"], t1=cfg["t1"], t2=cfg["t2"], warp=cfg["warp"], out=hlab_np)
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
     _barrier(world)
     t_e2e = _max_over_ranks(sum(e2e_ms) / len(e2e_ms), world)

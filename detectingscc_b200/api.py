@@ -103,8 +103,11 @@ class Engine:
         N.check(self._lib.scc_set_tuning(self._h, key.encode(), int(value)), f"scc_set_tuning({key})")
 
     def run(self, g: Graph, algo="h", t1=True, t2=True, warp=1, labels=True,
-            instrument=False, force=None) -> Result:
-        """Run on a host graph: the call copies the CSR in and the labels out."""
+            instrument=False, force=None, out: Optional[np.ndarray] = None) -> Result:
+        """Run on a host graph: the call copies the CSR in and the labels out.
+
+        out: optional preallocated host array (e.g. pinned) of V uint32.
+        """
         flags = (N.FLAG_TRIM1 if t1 else 0) | (N.FLAG_TRIM2 if t2 else 0)
         flags |= N.FLAG_INSTRUMENT if instrument else 0
         if force == "grid":
@@ -112,7 +115,10 @@ class Engine:
         elif force == "block":
             flags |= N.FLAG_FORCE_BLOCK
         view = N.CsrView(g.V, g.E, _ptr(g.Fr), _ptr(g.Fc), _ptr(g.Br), _ptr(g.Bc))
-        out = np.zeros(max(g.V, 1), dtype=np.uint32) if labels else None
+        if labels and out is None:
+            out = np.zeros(max(g.V, 1), dtype=np.uint32)
+        elif not labels:
+            out = None
         st = N.Stats()
         rc = self._lib.scc_run(self._h, ctypes.byref(view), _algo_code(algo), flags, int(warp),
                                _ptr(out), ctypes.byref(st), None)
