@@ -66,7 +66,7 @@ MAX_VERTICES = 268435454
 
 # every symbol include/scc_b200.h and include/scc_compat.h declare
 C_SYMBOLS = ["scc_create", "scc_destroy", "scc_run", "scc_set_tuning", "scc_status_string",
-             "scc_version", "scc_load_graph", "scc_save_binary", "scc_graph_from_arcs",
+             "scc_version", "scc_get_trace", "scc_load_graph", "scc_save_binary", "scc_graph_from_arcs",
              "scc_free_host_graph", "scc_reference_call", "scc_batch_create", "scc_batch_run",
              "scc_batch_destroy"]
 CXX_SYMBOLS = ["_Z5vHongjjPjS_S_S_bb", "_Z6vSlotajjPjS_S_S_bb", "_Z5wHongjjPjS_S_S_bbi",
@@ -115,6 +115,7 @@ def lib():
     L.scc_batch_run.argtypes = [vp, ctypes.c_int, u32, ctypes.c_int, vp, ctypes.POINTER(BatchResult),
                                 ctypes.POINTER(Stats)]
     L.scc_batch_destroy.argtypes = [vp]
+    L.scc_get_trace.argtypes = [vp, ctypes.POINTER(u64), u32, ctypes.POINTER(u32), ctypes.POINTER(u64)]
     _lib = L
     return L
 

@@ -102,6 +102,24 @@ class Engine:
     def set_tuning(self, key: str, value: int) -> None:
         N.check(self._lib.scc_set_tuning(self._h, key.encode(), int(value)), f"scc_set_tuning({key})")
 
+    PHASES = {1: "init", 2: "trim1_once", 3: "trim1_apply", 4: "trim1_fix", 5: "trim2", 6: "trim2_apply",
+              7: "first_pivot", 8: "bfs0", 9: "bfs", 10: "prop", 11: "hong_update", 12: "slota_first_update",
+              13: "slota_peel_update", 14: "rename", 15: "pivots", 16: "bfs_pull", 17: "prop_pull"}
+
+    def trace(self):
+        """Per-pass (phase, microseconds, items pushed) of the last run (needs set_tuning('trace', n))."""
+        n = ctypes.c_uint32(0)
+        t0 = ctypes.c_uint64(0)
+        N.check(self._lib.scc_get_trace(self._h, None, 0, ctypes.byref(n), ctypes.byref(t0)))
+        buf = (ctypes.c_uint64 * (2 * max(n.value, 1)))()
+        N.check(self._lib.scc_get_trace(self._h, buf, n.value, ctypes.byref(n), ctypes.byref(t0)))
+        out, prev = [], t0.value
+        for i in range(n.value):
+            t, info = buf[2 * i], buf[2 * i + 1]
+            out.append((self.PHASES.get(info & 0xFF, str(info & 0xFF)), (t - prev) / 1e3, info >> 8))
+            prev = t
+        return out
+
     def run(self, g: Graph, algo="h", t1=True, t2=True, warp=1, labels=True,
             instrument=False, force=None, out: Optional[np.ndarray] = None) -> Result:
         """Run on a host graph: the call copies the CSR in and the labels out.

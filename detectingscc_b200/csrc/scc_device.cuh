@@ -54,6 +54,16 @@ struct __align__(128) Ctl {
     unsigned long long timeout_ns;
     unsigned tail_pass;                            // pass at which CTA 0 took over (0 = never)
     unsigned nlive_tail;
+    unsigned long long t_start;                    // %globaltimer at kernel entry
+    unsigned long long *trace;                     // optional: 2 words per pass
+    unsigned trace_cap;
+};
+
+// Phase ids recorded in the pass trace.
+enum {
+    PH_INIT = 1, PH_TRIM1_ONCE = 2, PH_TRIM1_APPLY = 3, PH_TRIM1_FIX = 4, PH_TRIM2 = 5, PH_TRIM2_APPLY = 6,
+    PH_FIRST_PIVOT = 7, PH_BFS0 = 8, PH_BFS = 9, PH_PROP = 10, PH_HONG_UPDATE = 11, PH_SLOTA_FIRST_UPDATE = 12,
+    PH_SLOTA_PEEL_UPDATE = 13, PH_RENAME = 14, PH_PIVOTS = 15, PH_BFS_PULL = 16, PH_PROP_PULL = 17
 };
 
 struct Graph {
@@ -176,7 +186,7 @@ struct BlockExec {
 // counter slot gl%3 and buffer parity gl&1; the following pass reads them as
 // its "current" slot (gl+2)%3 and parity (gl+1)&1.
 template <class Ex, class F>
-__device__ __forceinline__ bool run_pass(Ex &ex, F &&body)
+__device__ __forceinline__ bool run_pass(Ex &ex, int phase, F &&body)
 {
     const unsigned nxt = ex.gl % 3u, clr = (ex.gl + 1u) % 3u, cur = (ex.gl + 2u) % 3u;
     if (ex.leader()) {
@@ -185,6 +195,14 @@ __device__ __forceinline__ bool run_pass(Ex &ex, F &&body)
     }
     body(cur, nxt);
     bool ok = ex.sync();
+    if (ex.leader() && ex.ctl->trace && ex.gl < ex.ctl->trace_cap) {
+        // pass trace: end time and (phase, items pushed) -- the reference's
+        // _DEBUG per-phase event timers (scc_WCC.cu:650-672) at pass granularity
+        const unsigned *c = ex.ctl->lc[nxt];
+        unsigned long long pushed = (unsigned long long)vld(&c[C_FQ]) + vld(&c[C_BQ]) + vld(&c[C_LIST]);
+        ex.ctl->trace[2 * ex.gl] = gtimer();
+        ex.ctl->trace[2 * ex.gl + 1] = (unsigned long long)phase | (pushed << 8);
+    }
     ex.gl++;
     return ok;
 }

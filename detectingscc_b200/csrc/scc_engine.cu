@@ -40,6 +40,7 @@ template <bool INSTR, bool HONG>
 __global__ void __launch_bounds__(GRID_THREADS, 2) k_scc_grid(Params p)
 {
     if (*(volatile int *)&p.w.ctl->error) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) p.w.ctl->t_start = gtimer();
     GridExec<INSTR> ex{p.w.ctl, 0u};
     Carry cy{0u, 0u, 0u};
     int rc = HONG ? hong_front(ex, p.g, p.w, p.t1, p.t2, p.lw, cy) : slota_front(ex, p.g, p.w, p.t1, p.lw, cy);
@@ -61,6 +62,7 @@ template <bool INSTR, bool HONG>
 __global__ void __launch_bounds__(BLOCK_THREADS, 1) k_scc_block(Params p)
 {
     if (*(volatile int *)&p.w.ctl->error) return;
+    if (threadIdx.x == 0) p.w.ctl->t_start = gtimer();
     BlockExec<INSTR> ex{p.w.ctl, 0u};
     Carry cy{0u, 0u, 0u};
     int rc = HONG ? hong_front(ex, p.g, p.w, p.t1, p.t2, p.lw, cy) : slota_front(ex, p.g, p.w, p.t1, p.lw, cy);
@@ -280,6 +282,8 @@ extern "C" int scc_destroy(scc_context *ctx)
     cudaFree(ctx->ws);
     cudaFree(ctx->dFr); cudaFree(ctx->dFc); cudaFree(ctx->dBr); cudaFree(ctx->dBc); cudaFree(ctx->dlab);
     if (ctx->hctl) cudaFreeHost(ctx->hctl);
+    cudaFree(ctx->dtrace);
+    if (ctx->htrace) cudaFreeHost(ctx->htrace);
     for (int i = 0; i < 4; i++) if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -350,6 +354,8 @@ extern "C" int scc_run(scc_context *ctx, const scc_csr_view *gv, int algo, uint3
     // control block: zeroed, then the timeout
     memset(ctx->hctl, 0, sizeof(Ctl));
     ctx->hctl->timeout_ns = (unsigned long long)ctx->timeout_ms * 1000000ull;
+    ctx->hctl->trace = ctx->dtrace;
+    ctx->hctl->trace_cap = ctx->dtrace ? ctx->trace_cap : 0u;
     CK(cudaMemcpyAsync(ctx->work.ctl, ctx->hctl, sizeof(Ctl), cudaMemcpyHostToDevice, st));
     CK(cudaMemsetAsync(ctx->work.pivkey, 0, hong ? (4 * ((size_t)V + 1) + 8) * 8 : 8, st));
 
@@ -387,6 +393,7 @@ extern "C" int scc_run(scc_context *ctx, const scc_csr_view *gv, int algo, uint3
         if (!dev) CK(cudaMemcpyAsync(labels_out, dout, (size_t)V * 4, cudaMemcpyDeviceToHost, st));
     }
     CK(cudaMemcpyAsync(ctx->hctl, ctx->work.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
+    if (ctx->dtrace) CK(cudaMemcpyAsync(ctx->htrace, ctx->dtrace, (size_t)ctx->trace_cap * 16, cudaMemcpyDeviceToHost, st));
     CK(cudaEventRecord(ctx->ev[3], st));
     CK(cudaStreamSynchronize(st));
     const Ctl &c = *ctx->hctl;
@@ -419,6 +426,33 @@ extern "C" int scc_set_tuning(scc_context *ctx, const char *key, long long value
     else if (!strcmp(key, "block_max_edges")) ctx->block_max_edges = (uint32_t)value;
     else if (!strcmp(key, "timeout_ms")) ctx->timeout_ms = (uint32_t)value;
     else if (!strcmp(key, "max_blocks_per_sm")) ctx->max_blocks_per_sm = (int)value;
-    else return SCC_ERR_INVALID_ARG;
+    else if (!strcmp(key, "trace")) {
+        // per-pass trace of the next runs: `value` passes (0 switches it off)
+        std::lock_guard<std::mutex> lock(ctx->mu);
+        cudaSetDevice(ctx->device);
+        cudaFree(ctx->dtrace);
+        cudaFreeHost(ctx->htrace);
+        ctx->dtrace = nullptr;
+        ctx->htrace = nullptr;
+        ctx->trace_cap = 0;
+        if (value > 0) {
+            if (cudaMalloc((void **)&ctx->dtrace, (size_t)value * 16) != cudaSuccess ||
+                cudaMallocHost((void **)&ctx->htrace, (size_t)value * 16) != cudaSuccess) {
+                cudaGetLastError();
+                return SCC_ERR_OOM;
+            }
+            ctx->trace_cap = (uint32_t)value;
+        }
+    } else return SCC_ERR_INVALID_ARG;
+    return SCC_OK;
+}
+
+extern "C" int scc_get_trace(scc_context *ctx, uint64_t *out, uint32_t cap, uint32_t *n_out, uint64_t *t_start)
+{
+    if (!ctx || !n_out) return SCC_ERR_INVALID_ARG;
+    uint32_t n = std::min<uint32_t>(ctx->hctl ? ctx->hctl->passes : 0u, ctx->trace_cap);
+    if (out && ctx->htrace) memcpy(out, ctx->htrace, (size_t)std::min(n, cap) * 16);
+    *n_out = n;
+    if (t_start) *t_start = ctx->hctl ? ctx->hctl->t_start : 0;
     return SCC_OK;
 }

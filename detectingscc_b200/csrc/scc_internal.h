@@ -32,6 +32,10 @@ struct scc_context {
     uint32_t timeout_ms = 4000;          // bound on any single grid-barrier wait
     int max_blocks_per_sm = 0;           // 0 = occupancy limit
 
+    // optional per-pass trace
+    unsigned long long *dtrace = nullptr, *htrace = nullptr;
+    uint32_t trace_cap = 0;
+
     std::mutex mu;
 };
 

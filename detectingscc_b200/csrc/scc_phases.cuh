@@ -99,7 +99,7 @@ __device__ __forceinline__ uint32_t trim2_partner(const Graph &g, const uint32_t
 template <class Ex>
 __device__ bool ph_init(Ex &ex, const Graph &g, const Work &w, bool fold_pivot)
 {
-    return run_pass(ex, [&](unsigned, unsigned) {
+    return run_pass(ex, PH_INIT, [&](unsigned, unsigned) {
         unsigned long long best = 0;
         for (uint32_t i = ex.tid(); i <= g.V; i += ex.nthr()) {
             w.st[i] = (i == 0u) ? DEAD : 0u;
@@ -121,7 +121,7 @@ __device__ bool ph_init(Ex &ex, const Graph &g, const Work &w, bool fold_pivot)
 template <class Ex>
 __device__ bool ph_trim1_once(Ex &ex, const Graph &g, const Work &w)
 {
-    bool ok = run_pass(ex, [&](unsigned, unsigned nxt) {
+    bool ok = run_pass(ex, PH_TRIM1_ONCE, [&](unsigned, unsigned nxt) {
         const unsigned par = ex.gl & 1u;
         unsigned long long best = 0;
         for (uint32_t base = ex.wid() * 32u; base < g.V; base += ex.nwarps() * 32u) {
@@ -145,7 +145,7 @@ __device__ bool ph_trim1_once(Ex &ex, const Graph &g, const Work &w)
     });
     if (!ok) return false;
     const uint32_t nT = last_count(ex, C_LIST);
-    return run_pass(ex, [&](unsigned, unsigned) {
+    return run_pass(ex, PH_TRIM1_APPLY, [&](unsigned, unsigned) {
         const uint32_t *T = w.Q[0][(ex.gl & 1u) ^ 1u];
         for (uint32_t i = ex.tid(); i < nT; i += ex.nthr()) {
             uint32_t v = T[i];
@@ -169,7 +169,7 @@ __device__ bool ph_trim1_fix(Ex &ex, const Graph &g, const Work &w, VList src0)
     bool first = true;
     for (unsigned it = 0;; it++) {
         if (it > g.V + 2u) { if (ex.leader()) set_error(ex.ctl, E_NOT_CONVERGED, 30); return false; }
-        bool ok = run_pass(ex, [&](unsigned, unsigned nxt) {
+        bool ok = run_pass(ex, PH_TRIM1_FIX, [&](unsigned, unsigned nxt) {
             const unsigned par = ex.gl & 1u;
             const uint32_t tag = ex.gl + 1u;
             VList src = first ? src0 : VList{w.Q[0][par ^ 1u], nq, 0u};
@@ -225,7 +225,7 @@ __device__ bool ph_trim1_fix(Ex &ex, const Graph &g, const Work &w, VList src0)
 template <class Ex>
 __device__ bool ph_trim2(Ex &ex, const Graph &g, const Work &w, VList src)
 {
-    bool ok = run_pass(ex, [&](unsigned, unsigned nxt) {
+    bool ok = run_pass(ex, PH_TRIM2, [&](unsigned, unsigned nxt) {
         const unsigned par = ex.gl & 1u;
         for (uint32_t base = ex.wid() * 32u; base < src.n; base += ex.nwarps() * 32u) {
             uint32_t i = base + lane_id();
@@ -250,7 +250,7 @@ __device__ bool ph_trim2(Ex &ex, const Graph &g, const Work &w, VList src)
     });
     if (!ok) return false;
     const uint32_t nT = last_count(ex, C_LIST);
-    return run_pass(ex, [&](unsigned, unsigned) {
+    return run_pass(ex, PH_TRIM2_APPLY, [&](unsigned, unsigned) {
         const uint32_t *T = w.Q[0][(ex.gl & 1u) ^ 1u];
         for (uint32_t i = ex.tid(); i < nT; i += ex.nthr()) w.st[T[i]] = DEAD;
     });
@@ -337,7 +337,7 @@ template <class Ex, class Seed>
 __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed seed, bool bw, int lw)
 {
     const unsigned gsz = (lw < 0) ? 32u : (32u >> lw);
-    bool ok = run_pass(ex, [&](unsigned, unsigned nxt) {
+    bool ok = run_pass(ex, PH_BFS0, [&](unsigned, unsigned nxt) {
         const unsigned par = ex.gl & 1u;
         const unsigned ng = (src.n + gsz - 1u) / gsz;
         const uint32_t bits = bw ? (FVB | BVB) : FVB;
@@ -364,7 +364,7 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
         const uint32_t nhf = last_count(ex, C_FH), nhb = last_count(ex, C_BH);
         if (nf + nb + nhf + nhb == 0u) return true;
         if (lev > g.V + 2u) { if (ex.leader()) set_error(ex.ctl, E_NOT_CONVERGED, 40); return false; }
-        ok = run_pass(ex, [&](unsigned, unsigned nxt) {
+        ok = run_pass(ex, PH_BFS, [&](unsigned, unsigned nxt) {
             const unsigned par = ex.gl & 1u, cp = par ^ 1u;
             const uint32_t ngf = (nf + gsz - 1u) / gsz, ngb = (nb + gsz - 1u) / gsz;
             const uint32_t nitems = nhf + nhb + ngf + ngb;
@@ -428,7 +428,7 @@ __device__ bool ph_propagate(Ex &ex, const Graph &g, const Work &w, VList src0)
     bool first = true;
     for (unsigned lev = 0;; lev++) {
         if (lev > g.V + 2u) { if (ex.leader()) set_error(ex.ctl, E_NOT_CONVERGED, 50); return false; }
-        bool ok = run_pass(ex, [&](unsigned, unsigned nxt) {
+        bool ok = run_pass(ex, PH_PROP, [&](unsigned, unsigned nxt) {
             const unsigned par = ex.gl & 1u, cp = par ^ 1u;
             const uint32_t tag = ex.gl + 1u;
             VList src = first ? src0 : VList{w.Q[0][cp], nq, 0u};
@@ -474,7 +474,7 @@ template <class Ex>
 __device__ bool ph_hong_update(Ex &ex, const Graph &g, const Work &w, VList src, uint32_t *Lout,
                                bool single, bool fold)
 {
-    return run_pass(ex, [&](unsigned, unsigned nxt) {
+    return run_pass(ex, PH_HONG_UPDATE, [&](unsigned, unsigned nxt) {
         for (uint32_t base = ex.wid() * 32u; base < src.n; base += ex.nwarps() * 32u) {
             uint32_t i = base + lane_id();
             bool valid = i < src.n, surv = false;
@@ -506,7 +506,7 @@ __device__ bool ph_hong_update(Ex &ex, const Graph &g, const Work &w, VList src,
 template <class Ex>
 __device__ bool ph_slota_first_update(Ex &ex, const Graph &g, const Work &w, uint32_t *Lout)
 {
-    return run_pass(ex, [&](unsigned, unsigned nxt) {
+    return run_pass(ex, PH_SLOTA_FIRST_UPDATE, [&](unsigned, unsigned nxt) {
         const uint32_t p = key_vertex(w.pivkey[0]);
         for (uint32_t base = ex.wid() * 32u; base < g.V; base += ex.nwarps() * 32u) {
             uint32_t v = base + lane_id() + 1u;
@@ -530,7 +530,7 @@ __device__ bool ph_slota_first_update(Ex &ex, const Graph &g, const Work &w, uin
 template <class Ex>
 __device__ bool ph_slota_peel_update(Ex &ex, const Graph &g, const Work &w, VList src, uint32_t *Lout)
 {
-    return run_pass(ex, [&](unsigned, unsigned nxt) {
+    return run_pass(ex, PH_SLOTA_PEEL_UPDATE, [&](unsigned, unsigned nxt) {
         for (uint32_t base = ex.wid() * 32u; base < src.n; base += ex.nwarps() * 32u) {
             uint32_t i = base + lane_id();
             bool valid = i < src.n, surv = false;
@@ -552,7 +552,7 @@ __device__ bool ph_slota_peel_update(Ex &ex, const Graph &g, const Work &w, VLis
 template <class Ex>
 __device__ bool ph_compact_rename(Ex &ex, const Graph &g, const Work &w, VList src, uint32_t *Lout)
 {
-    return run_pass(ex, [&](unsigned, unsigned nxt) {
+    return run_pass(ex, PH_RENAME, [&](unsigned, unsigned nxt) {
         for (uint32_t base = ex.wid() * 32u; base < src.n; base += ex.nwarps() * 32u) {
             uint32_t i = base + lane_id();
             bool valid = i < src.n, surv = false;
@@ -568,7 +568,7 @@ __device__ bool ph_compact_rename(Ex &ex, const Graph &g, const Work &w, VList s
 template <class Ex>
 __device__ bool ph_pivots(Ex &ex, const Graph &g, const Work &w, VList src)
 {
-    return run_pass(ex, [&](unsigned, unsigned) {
+    return run_pass(ex, PH_PIVOTS, [&](unsigned, unsigned) {
         for (uint32_t base = ex.wid() * 32u; base < src.n; base += ex.nwarps() * 32u) {
             uint32_t i = base + lane_id();
             bool valid = i < src.n;
@@ -614,7 +614,7 @@ __device__ int hong_loop(Ex &ex, const Graph &g, const Work &w, Carry &cy, uint3
 template <class Ex>
 __device__ bool ph_first_pivot(Ex &ex, const Graph &g, const Work &w)
 {
-    return run_pass(ex, [&](unsigned, unsigned) {
+    return run_pass(ex, PH_FIRST_PIVOT, [&](unsigned, unsigned) {
         unsigned long long best = 0;
         for (uint32_t v = ex.tid() + 1u; v <= g.V; v += ex.nthr()) {
             if (w.st[v] != DEAD) {

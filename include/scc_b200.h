@@ -112,8 +112,16 @@ int scc_run(scc_context *ctx, const scc_csr_view *g, int algo, uint32_t flags, i
  *   "block_max_vertices"  graphs up to this V run on the single-CTA path
  *   "block_max_edges"     ... and up to this E
  *   "timeout_ms"          bound on any grid-barrier wait (default 4000)
- *   "max_blocks_per_sm"   cap on CTAs per SM of the persistent launch */
+ *   "max_blocks_per_sm"   cap on CTAs per SM of the persistent launch
+ *   "trace"               record a per-pass trace of up to `value` passes */
 int scc_set_tuning(scc_context *ctx, const char *key, long long value);
+
+/* Per-pass trace of the last run (enable with scc_set_tuning(ctx, "trace",
+ * max_passes)): two words per pass, [2i] = %globaltimer (ns) at the end of
+ * pass i, [2i+1] = phase id | (items pushed << 8).  *n_out = passes
+ * recorded, *t_start = %globaltimer at kernel entry.  The reference keeps
+ * per-phase CUDA-event timers behind #define _DEBUG (scc_WCC.cu:650-672). */
+int scc_get_trace(scc_context *ctx, uint64_t *out, uint32_t cap, uint32_t *n_out, uint64_t *t_start);
 
 /* Human-readable text for a status code. */
 const char *scc_status_string(int status);
