@@ -149,7 +149,8 @@ class Engine:
         """Run on device-resident CSR (torch CUDA tensors or raw device pointers).
 
         labels_out: device buffer of V uint32/int32 entries, or None.
-        stream: a cudaStream_t handle (int) or None for the engine's stream.
+        stream: a cudaStream_t handle (int); None means the current PyTorch stream
+                of the tensors' device (or the engine's own stream for raw pointers).
         """
         flags = N.FLAG_DEVICE | (N.FLAG_TRIM1 if t1 else 0) | (N.FLAG_TRIM2 if t2 else 0)
         flags |= N.FLAG_INSTRUMENT if instrument else 0
@@ -157,6 +158,10 @@ class Engine:
             flags |= N.FLAG_FORCE_GRID
         elif force == "block":
             flags |= N.FLAG_FORCE_BLOCK
+        if stream is None and hasattr(Fr, "device") and getattr(Fr.device, "type", "") == "cuda":
+            # order after the producer of the tensors: run on their device's current stream
+            import torch
+            stream = torch.cuda.current_stream(Fr.device).cuda_stream
         view = N.CsrView(int(V), int(E), _ptr(Fr), _ptr(Fc), _ptr(Br), _ptr(Bc))
         st = N.Stats()
         rc = self._lib.scc_run(self._h, ctypes.byref(view), _algo_code(algo), flags, int(warp),

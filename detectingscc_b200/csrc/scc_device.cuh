@@ -79,7 +79,15 @@ struct Work {
     uint32_t hcap;
     unsigned long long *pivkey; // Hong: 4V+4 slots; Slota: 1
     Ctl *ctl;
+    uint32_t qcap;              // entries per CTA staging queue (dynamic shared memory)
+    uint32_t bu_den;            // bottom-up BFS when frontier > scope / bu_den (0 = never)
 };
+
+// Dynamic shared memory of the SCC kernels: 16 control words, then NBQ
+// staging queues of qcap entries each.
+constexpr unsigned NBQ = 2;
+constexpr unsigned BQ_WORDS = 16;
+extern __shared__ uint32_t sccb_dsmem[];
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
 __device__ __forceinline__ unsigned long long gtimer()
@@ -141,15 +149,14 @@ struct GridExec {
                 atomicExch(&ctl->bar_word, res);
             } else {
                 unsigned long long t0 = gtimer();
-                for (;;) {
+                for (unsigned spin = 1;; spin++) {
                     res = vld(&ctl->bar_word);
                     if ((res & 0x7FFFFFFFu) != (w0 & 0x7FFFFFFFu)) break;
-                    if (gtimer() - t0 > ctl->timeout_ns) {
+                    if ((spin & 255u) == 0u && gtimer() - t0 > ctl->timeout_ns) {
                         set_error(ctl, E_TIMEOUT, 1000);
                         res = 0x80000000u;
                         break;
                     }
-                    __nanosleep(64);
                 }
             }
             __threadfence();
@@ -234,6 +241,58 @@ __device__ __forceinline__ void warp_push(bool pred, uint32_t val, uint32_t *q, 
         unsigned pos = base + __popc(m & ((1u << lane) - 1u));
         if (pos < cap) q[pos] = val;
         else set_error(ctl, E_OVERFLOW, where);
+    }
+}
+
+// CTA-level staging of queue appends: lanes append into a shared-memory
+// buffer (one shared atomic per warp); bq_flush copies the buffer to the
+// global queue with one global atomicAdd per CTA and pass.  Appends beyond
+// the buffer go straight to the global queue.  This keeps the global queue
+// tail from becoming a same-address atomic hot spot (one per warp step).
+__device__ __forceinline__ void bq_init()
+{
+    if (threadIdx.x < BQ_WORDS) sccb_dsmem[threadIdx.x] = 0u;
+    __syncthreads();
+}
+
+__device__ __forceinline__ void bq_push(unsigned qi, bool pred, uint32_t val, uint32_t qcap, uint32_t *gq,
+                                        unsigned *gcnt, uint32_t gcap, Ctl *ctl, int where)
+{
+    unsigned m = __ballot_sync(FULL, pred);
+    if (m == 0u) return;
+    unsigned lane = lane_id();
+    unsigned ld = __ffs(m) - 1u;
+    unsigned base = 0;
+    if (lane == ld) base = atomicAdd(&sccb_dsmem[qi], (unsigned)__popc(m));
+    base = __shfl_sync(FULL, base, ld);
+    unsigned pos = base + __popc(m & ((1u << lane) - 1u));
+    bool spill = pred && pos >= qcap;
+    if (pred && !spill) sccb_dsmem[BQ_WORDS + qi * qcap + pos] = val;
+    warp_push(spill, val, gq, gcnt, gcap, ctl, where);
+}
+
+// Called by every thread of the CTA at the end of a pass.
+__device__ __forceinline__ void bq_flush(unsigned nq, uint32_t qcap, uint32_t *gq0, unsigned *gcnt0, uint32_t *gq1,
+                                         unsigned *gcnt1, uint32_t gcap, Ctl *ctl)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (unsigned qi = 0; qi < nq; qi++) {
+            unsigned n = min(sccb_dsmem[qi], qcap);
+            sccb_dsmem[4 + qi] = n;
+            sccb_dsmem[8 + qi] = n ? atomicAdd(qi ? gcnt1 : gcnt0, n) : 0u;
+            sccb_dsmem[qi] = 0u;
+        }
+    }
+    __syncthreads();
+    for (unsigned qi = 0; qi < nq; qi++) {
+        const unsigned n = sccb_dsmem[4 + qi], base = sccb_dsmem[8 + qi];
+        uint32_t *gq = qi ? gq1 : gq0;
+        const uint32_t *buf = &sccb_dsmem[BQ_WORDS + qi * qcap];
+        for (unsigned i = threadIdx.x; i < n; i += blockDim.x) {
+            if (base + i < gcap) gq[base + i] = buf[i];
+            else set_error(ctl, E_OVERFLOW, 3);
+        }
     }
 }
 

@@ -33,14 +33,17 @@ struct Params {
 // ---------------------------------------------------------------------
 // kernels
 // ---------------------------------------------------------------------
-constexpr int GRID_THREADS = 512;
+constexpr int GRID_THREADS = 1024;
 constexpr int BLOCK_THREADS = 1024;
 
+static size_t dyn_smem_bytes(uint32_t qcap) { return (BQ_WORDS + NBQ * (size_t)qcap) * sizeof(uint32_t); }
+
 template <bool INSTR, bool HONG>
-__global__ void __launch_bounds__(GRID_THREADS, 2) k_scc_grid(Params p)
+__global__ void __launch_bounds__(GRID_THREADS, 1) k_scc_grid(Params p)
 {
     if (*(volatile int *)&p.w.ctl->error) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) p.w.ctl->t_start = gtimer();
+    bq_init();
     GridExec<INSTR> ex{p.w.ctl, 0u};
     Carry cy{0u, 0u, 0u};
     int rc = HONG ? hong_front(ex, p.g, p.w, p.t1, p.t2, p.lw, cy) : slota_front(ex, p.g, p.w, p.t1, p.lw, cy);
@@ -63,6 +66,7 @@ __global__ void __launch_bounds__(BLOCK_THREADS, 1) k_scc_block(Params p)
 {
     if (*(volatile int *)&p.w.ctl->error) return;
     if (threadIdx.x == 0) p.w.ctl->t_start = gtimer();
+    bq_init();
     BlockExec<INSTR> ex{p.w.ctl, 0u};
     Carry cy{0u, 0u, 0u};
     int rc = HONG ? hong_front(ex, p.g, p.w, p.t1, p.t2, p.lw, cy) : slota_front(ex, p.g, p.w, p.t1, p.lw, cy);
@@ -290,10 +294,10 @@ extern "C" int scc_destroy(scc_context *ctx)
     return SCC_OK;
 }
 
-static int grid_blocks_for(scc_context *ctx, void *fn)
+static int grid_blocks_for(scc_context *ctx, void *fn, size_t smem)
 {
     int occ = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, GRID_THREADS, 0) != cudaSuccess) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, GRID_THREADS, smem) != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
@@ -364,6 +368,9 @@ extern "C" int scc_run(scc_context *ctx, const scc_csr_view *gv, int algo, uint3
     launches++;
     CK(cudaGetLastError());
 
+    ctx->work.qcap = ctx->qcap;
+    ctx->work.bu_den = ctx->bu_den;
+    const size_t smem = dyn_smem_bytes(ctx->qcap);
     Params p{g, ctx->work, (flags & SCC_FLAG_TRIM1) ? 1 : 0, (flags & SCC_FLAG_TRIM2) ? 1 : 0, lw, ctx->tail_vertices};
     bool use_block = (V <= ctx->block_max_vertices && E <= ctx->block_max_edges);
     if (flags & SCC_FLAG_FORCE_GRID) use_block = false;
@@ -373,14 +380,16 @@ extern "C" int scc_run(scc_context *ctx, const scc_csr_view *gv, int algo, uint3
     CK(cudaEventRecord(ctx->ev[1], st));
     if (use_block) {
         void *fn = pick_block(instr, hong);
+        CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         void *args[] = {&p};
-        CK(cudaLaunchKernel(fn, dim3(1), dim3(BLOCK_THREADS), args, 0, st));
+        CK(cudaLaunchKernel(fn, dim3(1), dim3(BLOCK_THREADS), args, smem, st));
     } else {
         void *fn = pick_grid(instr, hong);
-        nblocks = grid_blocks_for(ctx, fn);
+        CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        nblocks = grid_blocks_for(ctx, fn, smem);
         if (nblocks <= 0) return SCC_ERR_CUDA;
         void *args[] = {&p};
-        CK(cudaLaunchCooperativeKernel(fn, dim3(nblocks), dim3(GRID_THREADS), args, 0, st));
+        CK(cudaLaunchCooperativeKernel(fn, dim3(nblocks), dim3(GRID_THREADS), args, smem, st));
     }
     launches++;
     CK(cudaEventRecord(ctx->ev[2], st));
@@ -426,7 +435,11 @@ extern "C" int scc_set_tuning(scc_context *ctx, const char *key, long long value
     else if (!strcmp(key, "block_max_edges")) ctx->block_max_edges = (uint32_t)value;
     else if (!strcmp(key, "timeout_ms")) ctx->timeout_ms = (uint32_t)value;
     else if (!strcmp(key, "max_blocks_per_sm")) ctx->max_blocks_per_sm = (int)value;
-    else if (!strcmp(key, "trace")) {
+    else if (!strcmp(key, "bu_den")) ctx->bu_den = (uint32_t)value;
+    else if (!strcmp(key, "qcap")) {
+        if (value < 256 || value > 24576) return SCC_ERR_INVALID_ARG;
+        ctx->qcap = (uint32_t)value;
+    } else if (!strcmp(key, "trace")) {
         // per-pass trace of the next runs: `value` passes (0 switches it off)
         std::lock_guard<std::mutex> lock(ctx->mu);
         cudaSetDevice(ctx->device);

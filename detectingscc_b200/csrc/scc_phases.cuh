@@ -121,6 +121,9 @@ __device__ bool ph_init(Ex &ex, const Graph &g, const Work &w, bool fold_pivot)
 template <class Ex>
 __device__ bool ph_trim1_once(Ex &ex, const Graph &g, const Work &w)
 {
+    // Runs right after init, when every vertex is live in range 0: a vertex
+    // then has a live same-range in-neighbour iff its in-degree is non-zero
+    // (self-loops count, as in trim1), so the decision needs the offsets only.
     bool ok = run_pass(ex, PH_TRIM1_ONCE, [&](unsigned, unsigned nxt) {
         const unsigned par = ex.gl & 1u;
         unsigned long long best = 0;
@@ -128,20 +131,19 @@ __device__ bool ph_trim1_once(Ex &ex, const Graph &g, const Work &w)
             uint32_t v = base + lane_id() + 1u;
             bool valid = v <= g.V, trim = false;
             if (valid) {
-                uint32_t s = w.st[v];
-                if (s != DEAD) {
-                    uint32_t r = s & RMASK;
-                    trim = !has_live(ex, w.st, g.Br, g.Bc, v, r, g.V) || !has_live(ex, w.st, g.Fr, g.Fc, v, r, g.V);
-                    if (!trim) {
-                        unsigned long long k = pivot_key(g, v);
-                        best = k > best ? k : best;
-                    }
+                const uint32_t indeg = __ldg(&g.Br[v + 1]) - __ldg(&g.Br[v]);
+                const uint32_t outdeg = __ldg(&g.Fr[v + 1]) - __ldg(&g.Fr[v]);
+                trim = indeg == 0u || outdeg == 0u;
+                if (!trim) {
+                    unsigned long long k = ((unsigned long long)(outdeg * indeg) << 32) | (0xFFFFFFFFu - v);
+                    best = k > best ? k : best;
                 }
             }
             count_verts(ex, valid);
-            warp_push(trim, v, w.Q[0][par], &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 10);
+            bq_push(0, trim, v, w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 10);
         }
         block_max_atomic(best, &w.pivkey[0]);
+        bq_flush(1, w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_LIST], nullptr, nullptr, g.V, ex.ctl);
     });
     if (!ok) return false;
     const uint32_t nT = last_count(ex, C_LIST);
@@ -163,7 +165,7 @@ __device__ bool ph_trim1_once(Ex &ex, const Graph &g, const Work &w)
 // later passes only recheck vertices that lost a neighbour.
 // ---------------------------------------------------------------------
 template <class Ex>
-__device__ bool ph_trim1_fix(Ex &ex, const Graph &g, const Work &w, VList src0)
+__device__ bool ph_trim1_fix(Ex &ex, const Graph &g, const Work &w, VList src0, bool all_live)
 {
     uint32_t nq = 0;
     bool first = true;
@@ -181,7 +183,11 @@ __device__ bool ph_trim1_fix(Ex &ex, const Graph &g, const Work &w, VList src0)
                     uint32_t s = w.st[v];
                     if (s != DEAD) {
                         r = s & RMASK;
-                        trim = !has_live(ex, w.st, g.Br, g.Bc, v, r, g.V) || !has_live(ex, w.st, g.Fr, g.Fc, v, r, g.V);
+                        if (first && all_live)   // every vertex live in range 0: degrees decide
+                            trim = __ldg(&g.Br[v + 1]) == __ldg(&g.Br[v]) || __ldg(&g.Fr[v + 1]) == __ldg(&g.Fr[v]);
+                        else
+                            trim = !has_live(ex, w.st, g.Br, g.Bc, v, r, g.V) ||
+                                   !has_live(ex, w.st, g.Fr, g.Fc, v, r, g.V);
                         if (trim) { w.st[v] = DEAD; w.label[v] = v; }
                     }
                 }
@@ -202,12 +208,13 @@ __device__ bool ph_trim1_fix(Ex &ex, const Graph &g, const Work &w, VList src0)
                             bool ok2 = e < end, push = false;
                             uint32_t u = ok2 ? guard_id(__ldg(&C[e]), g.V, ex.ctl) : 0u;
                             if (ok2 && (w.st[u] & RMASK) == rj) push = stamp_claim(w.stamp, u, tag);
-                            warp_push(push, u, w.Q[0][par], &ex.ctl->lc[nxt][C_FQ], g.V, ex.ctl, 11);
+                            bq_push(0, push, u, w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_FQ], g.V, ex.ctl, 11);
                         }
                         count_edges(ex, end - beg);
                     }
                 }
             }
+            bq_flush(1, w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_FQ], nullptr, nullptr, g.V, ex.ctl);
         });
         if (!ok) return false;
         first = false;
@@ -245,8 +252,9 @@ __device__ bool ph_trim2(Ex &ex, const Graph &g, const Work &w, VList src)
             count_verts(ex, valid);
             unsigned m = __ballot_sync(FULL, cnt);
             if (lane_id() == 0 && m) atomicAdd(&ex.ctl->n_trim2, (unsigned long long)__popc(m));
-            warp_push(hit, v, w.Q[0][par], &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 12);
+            bq_push(0, hit, v, w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 12);
         }
+        bq_flush(1, w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_LIST], nullptr, nullptr, g.V, ex.ctl);
     });
     if (!ok) return false;
     const uint32_t nT = last_count(ex, C_LIST);
@@ -276,7 +284,7 @@ __device__ __forceinline__ void bfs_edge_visit(Ex &ex, const Graph &g, const Wor
         uint32_t s = w.st[nbr];
         if ((s & (RMASK | bit)) == r) claim = !(atomicOr(&w.st[nbr], bit) & bit);
     }
-    warp_push(claim, nbr, w.Q[dir][par], &ex.ctl->lc[nxt][C_FQ + dir], g.V, ex.ctl, 13);
+    bq_push((unsigned)dir, claim, nbr, w.qcap, w.Q[dir][par], &ex.ctl->lc[nxt][C_FQ + dir], g.V, ex.ctl, 13);
 }
 
 template <class Ex>
@@ -313,6 +321,60 @@ __device__ __forceinline__ void chunk_expand(Ex &ex, const uint32_t *__restrict_
     count_edges(ex, end > beg ? end - beg : 0u);
 }
 
+// Bottom-up step for one direction over 32 scope vertices (Beamer's
+// direction-optimizing BFS): an unvisited live vertex looks for a visited
+// neighbour of its own range among its in-neighbours (forward search) or
+// out-neighbours (backward search) and stops at the first one.  Lists up to
+// 32 entries are scanned by their lane; longer ones by the whole warp.
+template <class Ex>
+__device__ __forceinline__ void bfs_pull_group(Ex &ex, const Graph &g, const Work &w, int dir, VList scope,
+                                               uint32_t k, unsigned par, unsigned nxt)
+{
+    const uint32_t bit = dir ? BVB : FVB;
+    const uint32_t *R = dir ? g.Fr : g.Br;
+    const uint32_t *C = dir ? g.Fc : g.Bc;
+    const uint32_t i = k * 32u + lane_id();
+    const bool valid = i < scope.n;
+    const uint32_t v = valid ? scope.at(i) : 0u;
+    const uint32_t s = valid ? w.st[v] : DEAD;
+    const bool act = valid && s != DEAD && !(s & bit);
+    const uint32_t want = (s & RMASK) | bit;
+    uint32_t beg = 0, end = 0;
+    if (act) { beg = __ldg(&R[v]); end = __ldg(&R[v + 1]); }
+    bool found = false;
+    unsigned scanned = 0;
+    if (act && end - beg <= 32u) {
+        for (uint32_t e = beg; e < end; e++) {
+            scanned++;
+            if ((w.st[guard_id(__ldg(&C[e]), g.V, ex.ctl)] & (RMASK | bit)) == want) { found = true; break; }
+        }
+    }
+    unsigned hm = __ballot_sync(FULL, act && end - beg > 32u);
+    while (hm) {
+        const unsigned j = __ffs(hm) - 1u;
+        hm &= hm - 1u;
+        const uint32_t bj = __shfl_sync(FULL, beg, j), ej = __shfl_sync(FULL, end, j);
+        const uint32_t wj = __shfl_sync(FULL, want, j);
+        for (uint32_t b = bj; b < ej; b += 32u) {
+            const uint32_t e = b + lane_id();
+            const bool ok = e < ej;
+            const bool hit = ok && (w.st[guard_id(__ldg(&C[e]), g.V, ex.ctl)] & (RMASK | bit)) == wj;
+            if (lane_id() == 0) scanned += min(32u, ej - b);
+            if (__ballot_sync(FULL, hit)) {
+                if (lane_id() == j) found = true;
+                break;
+            }
+        }
+    }
+    if (found) atomicOr(&w.st[v], bit);
+    count_verts(ex, valid);
+    if constexpr (Ex::instr) {
+        unsigned t = __reduce_add_sync(FULL, scanned);
+        count_edges(ex, t);
+    }
+    bq_push((unsigned)dir, found, v, w.qcap, w.Q[dir][par], &ex.ctl->lc[nxt][C_FQ + dir], g.V, ex.ctl, 19);
+}
+
 // Seed predicates for the first BFS pass.
 struct SeedOne {      // the single first pivot
     uint32_t p;
@@ -330,11 +392,14 @@ struct SeedRoot {     // colouring roots (selectPivotColoring, scc_kernels.cu:56
 };
 
 // Forward (and backward) reachability to closure.  Pass 0 walks src, tests
-// the seed predicate, flags seeds and expands them; later passes expand the
-// frontier queues and the heavy chunks.  lw < 0 selects the load-balanced
-// warp schedule, lw >= 0 the virtual-warp schedule with W = 1 << lw.
+// the seed predicate, flags seeds and expands them.  Each later pass picks,
+// per direction, top-down (expand the frontier queue and the heavy chunks)
+// or bottom-up over `scope` (the vertices the search can reach) when the
+// frontier holds more than scope.n / bu_den vertices.  lw < 0 selects the
+// load-balanced warp schedule for top-down steps, lw >= 0 the virtual-warp
+// schedule with W = 1 << lw.
 template <class Ex, class Seed>
-__device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed seed, bool bw, int lw)
+__device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed seed, bool bw, int lw, VList scope)
 {
     const unsigned gsz = (lw < 0) ? 32u : (32u >> lw);
     bool ok = run_pass(ex, PH_BFS0, [&](unsigned, unsigned nxt) {
@@ -357,28 +422,37 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
             bfs_expand_lanes(ex, g, w, 0, v, act, r, lw, par, nxt);
             if (bw) bfs_expand_lanes(ex, g, w, 1, v, act, r, lw, par, nxt);
         }
+        bq_flush(2, w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_FQ], w.Q[1][par], &ex.ctl->lc[nxt][C_BQ], g.V, ex.ctl);
     });
     if (!ok) return false;
+    const uint32_t nsg = (scope.n + 31u) / 32u;
     for (unsigned lev = 1;; lev++) {
         const uint32_t nf = last_count(ex, C_FQ), nb = last_count(ex, C_BQ);
         const uint32_t nhf = last_count(ex, C_FH), nhb = last_count(ex, C_BH);
         if (nf + nb + nhf + nhb == 0u) return true;
         if (lev > g.V + 2u) { if (ex.leader()) set_error(ex.ctl, E_NOT_CONVERGED, 40); return false; }
-        ok = run_pass(ex, PH_BFS, [&](unsigned, unsigned nxt) {
+        const bool puf = w.bu_den && nf > scope.n / w.bu_den;
+        const bool pub = bw && w.bu_den && nb > scope.n / w.bu_den;
+        ok = run_pass(ex, (puf || pub) ? PH_BFS_PULL : PH_BFS, [&](unsigned, unsigned nxt) {
             const unsigned par = ex.gl & 1u, cp = par ^ 1u;
             const uint32_t ngf = (nf + gsz - 1u) / gsz, ngb = (nb + gsz - 1u) / gsz;
-            const uint32_t nitems = nhf + nhb + ngf + ngb;
-            for (uint32_t it = ex.wid(); it < nitems; it += ex.nwarps()) {
-                if (it < nhf + nhb) {
-                    int dir = it < nhf ? 0 : 1;
-                    uint2 hc = w.H[dir][cp][dir ? it - nhf : it];
+            const uint32_t items_f = puf ? nsg : nhf + ngf;
+            const uint32_t items_b = pub ? nsg : (bw ? nhb + ngb : 0u);
+            for (uint32_t it = ex.wid(); it < items_f + items_b; it += ex.nwarps()) {
+                const int dir = it < items_f ? 0 : 1;
+                const uint32_t k = dir ? it - items_f : it;
+                if (dir ? pub : puf) {
+                    bfs_pull_group(ex, g, w, dir, scope, k, par, nxt);
+                    continue;
+                }
+                const uint32_t nh = dir ? nhb : nhf;
+                if (k < nh) {
+                    uint2 hc = w.H[dir][cp][k];
                     uint32_t r = w.st[hc.x] & RMASK;
                     auto fn = [&](bool valid, uint32_t nbr, uint32_t rr) { bfs_edge_visit(ex, g, w, dir, valid, nbr, rr, par, nxt); };
                     chunk_expand(ex, dir ? g.Br : g.Fr, dir ? g.Bc : g.Fc, hc, r, fn);
                 } else {
-                    uint32_t gi = it - nhf - nhb;
-                    int dir = gi < ngf ? 0 : 1;
-                    if (dir) gi -= ngf;
+                    const uint32_t gi = k - nh;
                     const uint32_t n = dir ? nb : nf;
                     unsigned slot = (lw < 0) ? lane_id() : (lane_id() >> lw);
                     uint32_t i = gi * gsz + slot;
@@ -390,6 +464,8 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
                     bfs_expand_lanes(ex, g, w, dir, v, valid, r, lw, par, nxt);
                 }
             }
+            bq_flush(2, w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_FQ], w.Q[1][par], &ex.ctl->lc[nxt][C_BQ], g.V,
+                     ex.ctl);
         });
         if (!ok) return false;
     }
@@ -418,7 +494,7 @@ __device__ __forceinline__ void prop_visit(Ex &ex, const Graph &g, const Work &w
             if (s != DEAD && s > c) push = atomicMin(&w.st[u], c) > c && stamp_claim(w.stamp, u, tag);
         }
     }
-    warp_push(push, u, w.Q[0][par], &ex.ctl->lc[nxt][C_FQ], g.V, ex.ctl, 14);
+    bq_push(0, push, u, w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_FQ], g.V, ex.ctl, 14);
 }
 
 template <bool MAXP, class Ex>
@@ -454,6 +530,7 @@ __device__ bool ph_propagate(Ex &ex, const Graph &g, const Work &w, VList src0)
                     count_edges(ex, lbs_expand(beg, deg, c, g.Bc, fn));
                 }
             }
+            bq_flush(1, w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_FQ], nullptr, nullptr, g.V, ex.ctl);
         });
         if (!ok) return false;
         first = false;
@@ -494,9 +571,10 @@ __device__ bool ph_hong_update(Ex &ex, const Graph &g, const Work &w, VList src,
                 }
             }
             count_verts(ex, valid);
-            warp_push(surv, v, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 15);
+            bq_push(0, surv, v, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 15);
             if (fold) range_max_atomic(surv, nr, surv ? pivot_key(g, v) : 0ull, w.pivkey);
         }
+        bq_flush(1, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], nullptr, nullptr, g.V, ex.ctl);
     });
 }
 
@@ -519,8 +597,9 @@ __device__ bool ph_slota_first_update(Ex &ex, const Graph &g, const Work &w, uin
                 }
             }
             count_verts(ex, valid);
-            warp_push(surv, v, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 16);
+            bq_push(0, surv, v, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 16);
         }
+        bq_flush(1, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], nullptr, nullptr, g.V, ex.ctl);
     });
 }
 
@@ -541,8 +620,9 @@ __device__ bool ph_slota_peel_update(Ex &ex, const Graph &g, const Work &w, VLis
                 else { w.st[v] = v; surv = true; }
             }
             count_verts(ex, valid);
-            warp_push(surv, v, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 17);
+            bq_push(0, surv, v, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 17);
         }
+        bq_flush(1, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], nullptr, nullptr, g.V, ex.ctl);
     });
 }
 
@@ -559,8 +639,9 @@ __device__ bool ph_compact_rename(Ex &ex, const Graph &g, const Work &w, VList s
             uint32_t v = valid ? src.at(i) : 0u;
             if (valid && w.st[v] != DEAD) { w.st[v] = v; surv = true; }
             count_verts(ex, valid);
-            warp_push(surv, v, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 18);
+            bq_push(0, surv, v, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 18);
         }
+        bq_flush(1, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], nullptr, nullptr, g.V, ex.ctl);
     });
 }
 
@@ -600,7 +681,7 @@ __device__ int hong_loop(Ex &ex, const Graph &g, const Work &w, Carry &cy, uint3
         if (Ex::grid && cy.nL <= tail_n) { cy.gl = ex.gl; return RUN_SWITCH; }
         if (ex.leader()) ex.ctl->outer++;
         const VList L{w.L[cy.lsel], cy.nL, 0u};
-        if (!ph_bfs(ex, g, w, L, SeedPivkey{}, true, -1)) return RUN_ERROR;
+        if (!ph_bfs(ex, g, w, L, SeedPivkey{}, true, -1, L)) return RUN_ERROR;
         if (!ph_hong_update(ex, g, w, L, w.L[cy.lsel ^ 1u], false, true)) return RUN_ERROR;
         cy.nL = last_count(ex, C_LIST);
         cy.lsel ^= 1u;
@@ -639,7 +720,7 @@ __device__ bool first_fwbw(Ex &ex, const Graph &g, const Work &w, int lw)
 {
     const unsigned long long k = vld64(&w.pivkey[0]);
     const uint32_t p = k ? key_vertex(k) : 0u;
-    return ph_bfs(ex, g, w, VList{nullptr, k ? 1u : 0u, p}, SeedOne{p}, true, lw);
+    return ph_bfs(ex, g, w, VList{nullptr, k ? 1u : 0u, p}, SeedOne{p}, true, lw, VList{nullptr, g.V, 1u});
 }
 
 // vHong / wHong up to the main loop (scc_WCC.cu:573-848): trim1*, first
@@ -650,15 +731,15 @@ __device__ int hong_front(Ex &ex, const Graph &g, const Work &w, bool t1, bool t
     const VList all{nullptr, g.V, 1u};
     if (!ph_init(ex, g, w, !t1)) return RUN_ERROR;
     if (t1) {
-        if (!ph_trim1_fix(ex, g, w, all)) return RUN_ERROR;
+        if (!ph_trim1_fix(ex, g, w, all, true)) return RUN_ERROR;
         if (!ph_first_pivot(ex, g, w)) return RUN_ERROR;
     }
     if (!first_fwbw(ex, g, w, lw)) return RUN_ERROR;
     if (!ph_hong_update(ex, g, w, all, w.L[0], true, false)) return RUN_ERROR;
     uint32_t n0 = last_count(ex, C_LIST);
-    if (t1 && !ph_trim1_fix(ex, g, w, VList{w.L[0], n0, 0u})) return RUN_ERROR;
+    if (t1 && !ph_trim1_fix(ex, g, w, VList{w.L[0], n0, 0u}, false)) return RUN_ERROR;
     if (t2 && !ph_trim2(ex, g, w, VList{w.L[0], n0, 0u})) return RUN_ERROR;
-    if (t1 && t2 && !ph_trim1_fix(ex, g, w, VList{w.L[0], n0, 0u})) return RUN_ERROR;
+    if (t1 && t2 && !ph_trim1_fix(ex, g, w, VList{w.L[0], n0, 0u}, false)) return RUN_ERROR;
     if (!ph_compact_rename(ex, g, w, VList{w.L[0], n0, 0u}, w.L[1])) return RUN_ERROR;
     cy.lsel = 1u;
     cy.nL = last_count(ex, C_LIST);
@@ -695,7 +776,7 @@ __device__ int slota_peels(Ex &ex, const Graph &g, const Work &w, Carry &cy, uin
         if (ex.leader()) ex.ctl->outer++;
         const VList L{w.L[cy.lsel], cy.nL, 0u};
         if (!ph_propagate<true>(ex, g, w, L)) return RUN_ERROR;
-        if (!ph_bfs(ex, g, w, L, SeedRoot{}, false, -1)) return RUN_ERROR;
+        if (!ph_bfs(ex, g, w, L, SeedRoot{}, false, -1, L)) return RUN_ERROR;
         if (!ph_slota_peel_update(ex, g, w, L, w.L[cy.lsel ^ 1u])) return RUN_ERROR;
         cy.nL = last_count(ex, C_LIST);
         cy.lsel ^= 1u;
