@@ -140,7 +140,7 @@ class Engine:
         st = N.Stats()
         rc = self._lib.scc_run(self._h, ctypes.byref(view), _algo_code(algo), flags, int(warp),
                                _ptr(out), ctypes.byref(st), None)
-        N.check(rc, "scc_run")
+        N.check(rc, f"scc_run (device error location {st.error_where})" if rc else "scc_run")
         return Result(out[:g.V] if labels else None, st.num_sccs, st.num_trim1, st.num_trim2,
                       st.num_pivot, st.as_dict())
 
@@ -166,7 +166,7 @@ class Engine:
         st = N.Stats()
         rc = self._lib.scc_run(self._h, ctypes.byref(view), _algo_code(algo), flags, int(warp),
                                _ptr(labels_out), ctypes.byref(st), stream)
-        N.check(rc, "scc_run")
+        N.check(rc, f"scc_run (device error location {st.error_where})" if rc else "scc_run")
         return Result(None, st.num_sccs, st.num_trim1, st.num_trim2, st.num_pivot, st.as_dict())
 
 
