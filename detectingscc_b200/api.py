@@ -150,7 +150,7 @@ class Engine:
 
         labels_out: device buffer of V uint32/int32 entries, or None.
         stream: a cudaStream_t handle (int); None means the current PyTorch stream
-                of the tensors' device (or the engine's own stream for raw pointers).
+                of the tensors' device (or the legacy default stream for raw pointers).
         """
         flags = N.FLAG_DEVICE | (N.FLAG_TRIM1 if t1 else 0) | (N.FLAG_TRIM2 if t2 else 0)
         flags |= N.FLAG_INSTRUMENT if instrument else 0

@@ -44,9 +44,11 @@ constexpr int E_BAD_GRAPH = 23;
 enum { C_FQ = 0, C_BQ = 1, C_FH = 2, C_BH = 3, C_LIST = 4, C_AUX = 5, NCNT = 8 };
 
 struct __align__(128) Ctl {
-    unsigned bar_count; unsigned _p0[31];
-    unsigned bar_word; unsigned _p1[31];          // generation (bits 0..30) | error (bit 31)
-    int error; int where; unsigned _p2[30];
+    // grid barrier arrival counter and the sticky error code share one
+    // 8-byte word so that a waiter polls both with one load
+    unsigned bar_count;
+    int error;
+    int where; unsigned _p0[29];
     unsigned lc[3][NCNT]; unsigned _p3[8];         // per-pass counters, 3-slot ring
     unsigned long long n_trim1, n_trim2, n_pivot;
     unsigned long long t_edges, t_verts;           // instrumented work counters
@@ -129,41 +131,41 @@ struct GridExec {
     __device__ __forceinline__ unsigned nwarps() const { return nthr() >> 5; }
     __device__ __forceinline__ bool leader() const { return blockIdx.x == 0 && threadIdx.x == 0; }
 
-    // Grid barrier.  The releasing CTA folds the error flag into the
-    // generation word so that every CTA takes the same decision; a waiter
-    // gives up after ctl->timeout_ns and reports E_TIMEOUT.
+    // Grid barrier.  One arrival counter: CTA 0 adds 0x80000000 - (n - 1),
+    // every other CTA adds 1, so bit 31 flips exactly when all n CTAs have
+    // arrived.  Arrival is a release, the flip is read with acquire.  A
+    // waiter leaves early when the sticky error word (polled with the
+    // counter in one 8-byte load) is set, or after ctl->timeout_ns; any CTA
+    // that sees an error returns, and the error stays set for the others.
     __device__ bool sync()
     {
-        __shared__ unsigned s_word;
+        __shared__ int s_err;
         __syncthreads();
         if (threadIdx.x == 0) {
-            unsigned w0 = vld(&ctl->bar_word);
-            __threadfence();
-            unsigned arrived = atomicAdd(&ctl->bar_count, 1u);
-            unsigned res;
-            if (arrived == gridDim.x - 1) {
-                atomicExch(&ctl->bar_count, 0u);
-                int err = *(volatile int *)&ctl->error;
-                res = ((w0 + 1u) & 0x7FFFFFFFu) | (err ? 0x80000000u : 0u);
-                __threadfence();
-                atomicExch(&ctl->bar_word, res);
-            } else {
-                unsigned long long t0 = gtimer();
-                for (unsigned spin = 1;; spin++) {
-                    res = vld(&ctl->bar_word);
-                    if ((res & 0x7FFFFFFFu) != (w0 & 0x7FFFFFFFu)) break;
-                    if ((spin & 255u) == 0u && gtimer() - t0 > ctl->timeout_ns) {
+            const unsigned nb = (blockIdx.x == 0) ? (0x80000000u - (gridDim.x - 1u)) : 1u;
+            unsigned old;
+            asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(&ctl->bar_count), "r"(nb) : "memory");
+            int err = 0;
+            unsigned long long t0 = 0;
+            for (unsigned spin = 0;; spin++) {
+                unsigned long long wv;
+                asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(wv) : "l"(&ctl->bar_count) : "memory");
+                err = (int)(wv >> 32);
+                if ((((unsigned)wv ^ old) & 0x80000000u) != 0u || err) break;
+                if ((spin & 255u) == 0u) {
+                    unsigned long long t = gtimer();
+                    if (spin == 0) t0 = t;
+                    else if (t - t0 > ctl->timeout_ns) {
                         set_error(ctl, E_TIMEOUT, 1000);
-                        res = 0x80000000u;
+                        err = E_TIMEOUT;
                         break;
                     }
                 }
             }
-            __threadfence();
-            s_word = res;
+            s_err = err;
         }
         __syncthreads();
-        return !(s_word & 0x80000000u);
+        return s_err == 0;
     }
 };
 

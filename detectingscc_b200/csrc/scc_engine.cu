@@ -333,7 +333,9 @@ extern "C" int scc_run(scc_context *ctx, const scc_csr_view *gv, int algo, uint3
     const bool instr = (flags & SCC_FLAG_INSTRUMENT) != 0;
     std::lock_guard<std::mutex> lock(ctx->mu);
     CK(cudaSetDevice(ctx->device));
-    cudaStream_t st = stream_arg ? (cudaStream_t)stream_arg : ctx->stream;
+    // NULL is the legacy default stream, as everywhere in CUDA (it is also
+    // the handle a PyTorch "current stream" has unless the caller set one)
+    cudaStream_t st = (cudaStream_t)stream_arg;
     int rc = scc_ctx_reserve(ctx, V, E);
     if (rc != SCC_OK) return rc;
     unsigned launches = 0;

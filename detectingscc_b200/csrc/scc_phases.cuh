@@ -119,42 +119,39 @@ __device__ bool ph_init(Ex &ex, const Graph &g, const Work &w, bool fold_pivot)
 // key on the way (pollForFirstPivot, scc_kernels.cu:643-656).
 // ---------------------------------------------------------------------
 template <class Ex>
-__device__ bool ph_trim1_once(Ex &ex, const Graph &g, const Work &w)
+__device__ bool ph_trim1_once(Ex &ex, const Graph &g, const Work &w, uint32_t *Lout)
 {
     // Runs right after init, when every vertex is live in range 0: a vertex
     // then has a live same-range in-neighbour iff its in-degree is non-zero
-    // (self-loops count, as in trim1), so the decision needs the offsets only.
-    bool ok = run_pass(ex, PH_TRIM1_ONCE, [&](unsigned, unsigned nxt) {
-        const unsigned par = ex.gl & 1u;
+    // (self-loops count, as in trim1), so the decision reads the offsets
+    // only and the pass can mark vertices as it goes.  Survivors are
+    // compacted into Lout and bid for the first pivot.
+    return run_pass(ex, PH_TRIM1_ONCE, [&](unsigned, unsigned nxt) {
         unsigned long long best = 0;
+        unsigned ntrim = 0;
         for (uint32_t base = ex.wid() * 32u; base < g.V; base += ex.nwarps() * 32u) {
             uint32_t v = base + lane_id() + 1u;
-            bool valid = v <= g.V, trim = false;
+            bool valid = v <= g.V, surv = false;
             if (valid) {
                 const uint32_t indeg = __ldg(&g.Br[v + 1]) - __ldg(&g.Br[v]);
                 const uint32_t outdeg = __ldg(&g.Fr[v + 1]) - __ldg(&g.Fr[v]);
-                trim = indeg == 0u || outdeg == 0u;
-                if (!trim) {
+                if (indeg == 0u || outdeg == 0u) {
+                    w.st[v] = DEAD;
+                    w.label[v] = v;
+                    ntrim++;
+                } else {
+                    surv = true;
                     unsigned long long k = ((unsigned long long)(outdeg * indeg) << 32) | (0xFFFFFFFFu - v);
                     best = k > best ? k : best;
                 }
             }
             count_verts(ex, valid);
-            bq_push(0, trim, v, w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 10);
+            bq_push(0, surv, v, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 10);
         }
+        ntrim = __reduce_add_sync(FULL, ntrim);
+        if (lane_id() == 0 && ntrim) atomicAdd(&ex.ctl->n_trim1, (unsigned long long)ntrim);
         block_max_atomic(best, &w.pivkey[0]);
-        bq_flush(1, w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_LIST], nullptr, nullptr, g.V, ex.ctl);
-    });
-    if (!ok) return false;
-    const uint32_t nT = last_count(ex, C_LIST);
-    return run_pass(ex, PH_TRIM1_APPLY, [&](unsigned, unsigned) {
-        const uint32_t *T = w.Q[0][(ex.gl & 1u) ^ 1u];
-        for (uint32_t i = ex.tid(); i < nT; i += ex.nthr()) {
-            uint32_t v = T[i];
-            w.st[v] = DEAD;
-            w.label[v] = v;
-        }
-        if (ex.leader()) ex.ctl->n_trim1 += nT;
+        bq_flush(1, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], nullptr, nullptr, g.V, ex.ctl);
     });
 }
 
@@ -402,10 +399,29 @@ template <class Ex, class Seed>
 __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed seed, bool bw, int lw, VList scope)
 {
     const unsigned gsz = (lw < 0) ? 32u : (32u >> lw);
+    const bool single = src.n == 1u && src.p == nullptr;
     bool ok = run_pass(ex, PH_BFS0, [&](unsigned, unsigned nxt) {
         const unsigned par = ex.gl & 1u;
-        const unsigned ng = (src.n + gsz - 1u) / gsz;
+        const unsigned ng = single ? 0u : (src.n + gsz - 1u) / gsz;
         const uint32_t bits = bw ? (FVB | BVB) : FVB;
+        if (single && seed(w, src.base)) {
+            // one seed (the first pivot, usually the largest hub): every warp
+            // takes CH-entry chunks of its out- and in-list in this pass
+            const uint32_t p = src.base;
+            if (ex.leader()) {
+                atomicOr(&w.st[p], bits);
+                atomicAdd(&ex.ctl->n_pivot, 1ull);
+            }
+            const uint32_t r = w.st[p] & RMASK;
+            const uint32_t nfc = (__ldg(&g.Fr[p + 1]) - __ldg(&g.Fr[p]) + CH - 1u) / CH;
+            const uint32_t nbc = bw ? (__ldg(&g.Br[p + 1]) - __ldg(&g.Br[p]) + CH - 1u) / CH : 0u;
+            for (uint32_t c = ex.wid(); c < nfc + nbc; c += ex.nwarps()) {
+                const int dir = c < nfc ? 0 : 1;
+                const uint2 hc = make_uint2(p, dir ? c - nfc : c);
+                auto fn = [&](bool valid, uint32_t nbr, uint32_t rr) { bfs_edge_visit(ex, g, w, dir, valid, nbr, rr, par, nxt); };
+                chunk_expand(ex, dir ? g.Br : g.Fr, dir ? g.Bc : g.Fc, hc, r, fn);
+            }
+        }
         for (uint32_t it = ex.wid(); it < ng; it += ex.nwarps()) {
             unsigned slot = (lw < 0) ? lane_id() : (lane_id() >> lw);
             uint32_t i = it * gsz + slot;
@@ -582,13 +598,14 @@ __device__ bool ph_hong_update(Ex &ex, const Graph &g, const Work &w, VList src,
 // the colouring with colour = its own id (assignUniqueRange,
 // scc_kernels.cu:477-484) and is appended to the live list.
 template <class Ex>
-__device__ bool ph_slota_first_update(Ex &ex, const Graph &g, const Work &w, uint32_t *Lout)
+__device__ bool ph_slota_first_update(Ex &ex, const Graph &g, const Work &w, VList src, uint32_t *Lout)
 {
     return run_pass(ex, PH_SLOTA_FIRST_UPDATE, [&](unsigned, unsigned nxt) {
         const uint32_t p = key_vertex(w.pivkey[0]);
-        for (uint32_t base = ex.wid() * 32u; base < g.V; base += ex.nwarps() * 32u) {
-            uint32_t v = base + lane_id() + 1u;
-            bool valid = v <= g.V, surv = false;
+        for (uint32_t base = ex.wid() * 32u; base < src.n; base += ex.nwarps() * 32u) {
+            uint32_t i = base + lane_id();
+            bool valid = i < src.n, surv = false;
+            uint32_t v = valid ? src.at(i) : 0u;
             if (valid) {
                 uint32_t s = w.st[v];
                 if (s != DEAD) {
@@ -691,19 +708,25 @@ __device__ int hong_loop(Ex &ex, const Graph &g, const Work &w, Carry &cy, uint3
 }
 
 // First pivot over the live vertices after trim1 to fixpoint
-// (pollForFirstPivot / selectFirstPivot, scc_WCC.cu:701-703).
+// (pollForFirstPivot / selectFirstPivot, scc_WCC.cu:701-703); the live
+// vertices are compacted into Lout on the way.
 template <class Ex>
-__device__ bool ph_first_pivot(Ex &ex, const Graph &g, const Work &w)
+__device__ bool ph_first_pivot(Ex &ex, const Graph &g, const Work &w, uint32_t *Lout)
 {
-    return run_pass(ex, PH_FIRST_PIVOT, [&](unsigned, unsigned) {
+    return run_pass(ex, PH_FIRST_PIVOT, [&](unsigned, unsigned nxt) {
         unsigned long long best = 0;
-        for (uint32_t v = ex.tid() + 1u; v <= g.V; v += ex.nthr()) {
-            if (w.st[v] != DEAD) {
+        for (uint32_t base = ex.wid() * 32u; base < g.V; base += ex.nwarps() * 32u) {
+            const uint32_t v = base + lane_id() + 1u;
+            const bool live = v <= g.V && w.st[v] != DEAD;
+            if (live) {
                 unsigned long long k = pivot_key(g, v);
                 best = k > best ? k : best;
             }
+            count_verts(ex, v <= g.V);
+            bq_push(0, live, v, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 20);
         }
         block_max_atomic(best, &w.pivkey[0]);
+        bq_flush(1, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], nullptr, nullptr, g.V, ex.ctl);
     });
 }
 
@@ -716,11 +739,11 @@ __device__ __forceinline__ unsigned long long vld64(const unsigned long long *p)
 // (scc_WCC.cu:717-743, scc_Coloring.cu:539-565; wHong / wSlota run it with
 // the virtual-warp schedule, scc_WCC.cu:209-317, scc_Coloring.cu:154-263).
 template <class Ex>
-__device__ bool first_fwbw(Ex &ex, const Graph &g, const Work &w, int lw)
+__device__ bool first_fwbw(Ex &ex, const Graph &g, const Work &w, int lw, VList scope)
 {
     const unsigned long long k = vld64(&w.pivkey[0]);
     const uint32_t p = k ? key_vertex(k) : 0u;
-    return ph_bfs(ex, g, w, VList{nullptr, k ? 1u : 0u, p}, SeedOne{p}, true, lw, VList{nullptr, g.V, 1u});
+    return ph_bfs(ex, g, w, VList{nullptr, k ? 1u : 0u, p}, SeedOne{p}, true, lw, scope);
 }
 
 // vHong / wHong up to the main loop (scc_WCC.cu:573-848): trim1*, first
@@ -729,21 +752,23 @@ template <class Ex>
 __device__ int hong_front(Ex &ex, const Graph &g, const Work &w, bool t1, bool t2, int lw, Carry &cy)
 {
     const VList all{nullptr, g.V, 1u};
+    VList scope = all;
     if (!ph_init(ex, g, w, !t1)) return RUN_ERROR;
     if (t1) {
         if (!ph_trim1_fix(ex, g, w, all, true)) return RUN_ERROR;
-        if (!ph_first_pivot(ex, g, w)) return RUN_ERROR;
+        if (!ph_first_pivot(ex, g, w, w.L[0])) return RUN_ERROR;
+        scope = VList{w.L[0], last_count(ex, C_LIST), 0u};
     }
-    if (!first_fwbw(ex, g, w, lw)) return RUN_ERROR;
-    if (!ph_hong_update(ex, g, w, all, w.L[0], true, false)) return RUN_ERROR;
-    uint32_t n0 = last_count(ex, C_LIST);
-    if (t1 && !ph_trim1_fix(ex, g, w, VList{w.L[0], n0, 0u}, false)) return RUN_ERROR;
-    if (t2 && !ph_trim2(ex, g, w, VList{w.L[0], n0, 0u})) return RUN_ERROR;
-    if (t1 && t2 && !ph_trim1_fix(ex, g, w, VList{w.L[0], n0, 0u}, false)) return RUN_ERROR;
-    if (!ph_compact_rename(ex, g, w, VList{w.L[0], n0, 0u}, w.L[1])) return RUN_ERROR;
-    cy.lsel = 1u;
+    if (!first_fwbw(ex, g, w, lw, scope)) return RUN_ERROR;
+    if (!ph_hong_update(ex, g, w, scope, w.L[1], true, false)) return RUN_ERROR;
+    const VList L1{w.L[1], last_count(ex, C_LIST), 0u};
+    if (t1 && !ph_trim1_fix(ex, g, w, L1, false)) return RUN_ERROR;
+    if (t2 && !ph_trim2(ex, g, w, L1)) return RUN_ERROR;
+    if (t1 && t2 && !ph_trim1_fix(ex, g, w, L1, false)) return RUN_ERROR;
+    if (!ph_compact_rename(ex, g, w, L1, w.L[0])) return RUN_ERROR;
+    cy.lsel = 0u;
     cy.nL = last_count(ex, C_LIST);
-    const VList L{w.L[1], cy.nL, 0u};
+    const VList L{w.L[0], cy.nL, 0u};
     if (!ph_propagate<false>(ex, g, w, L)) return RUN_ERROR;
     if (!ph_pivots(ex, g, w, L)) return RUN_ERROR;
     cy.gl = ex.gl;
@@ -756,11 +781,15 @@ __device__ int hong_front(Ex &ex, const Graph &g, const Work &w, bool t1, bool t
 template <class Ex>
 __device__ int slota_front(Ex &ex, const Graph &g, const Work &w, bool t1, int lw, Carry &cy)
 {
+    VList scope{nullptr, g.V, 1u};
     if (!ph_init(ex, g, w, !t1)) return RUN_ERROR;
-    if (t1 && !ph_trim1_once(ex, g, w)) return RUN_ERROR;
-    if (!first_fwbw(ex, g, w, lw)) return RUN_ERROR;
-    if (!ph_slota_first_update(ex, g, w, w.L[0])) return RUN_ERROR;
-    cy.lsel = 0u;
+    if (t1) {
+        if (!ph_trim1_once(ex, g, w, w.L[0])) return RUN_ERROR;
+        scope = VList{w.L[0], last_count(ex, C_LIST), 0u};
+    }
+    if (!first_fwbw(ex, g, w, lw, scope)) return RUN_ERROR;
+    if (!ph_slota_first_update(ex, g, w, scope, w.L[1])) return RUN_ERROR;
+    cy.lsel = 1u;
     cy.nL = last_count(ex, C_LIST);
     cy.gl = ex.gl;
     return RUN_DONE;

@@ -97,7 +97,8 @@ int scc_destroy(scc_context *ctx);
  *   labels_out  V entries or NULL: labels_out[i] = smallest vertex id of
  *               the SCC of vertex i+1 (1-based ids, canonical labels)
  *   stats       optional
- *   stream      cudaStream_t to run on, or NULL for the context's stream
+ *   stream      cudaStream_t to run on; NULL is the legacy default stream.
+ *               Device inputs must be complete in that stream's order.
  * With SCC_FLAG_DEVICE the CSR arrays and labels_out are device pointers;
  * otherwise they are host pointers and the call copies them.  Synchronous:
  * returns after the result (and the labels) are complete.
