@@ -68,7 +68,7 @@ MAX_VERTICES = 268435454
 C_SYMBOLS = ["scc_create", "scc_destroy", "scc_run", "scc_set_tuning", "scc_status_string",
              "scc_version", "scc_get_trace", "scc_load_graph", "scc_save_binary", "scc_graph_from_arcs",
              "scc_free_host_graph", "scc_reference_call", "scc_batch_create", "scc_batch_run",
-             "scc_batch_destroy"]
+             "scc_batch_destroy", "scc_run_noalloc"]
 CXX_SYMBOLS = ["_Z5vHongjjPjS_S_S_bb", "_Z6vSlotajjPjS_S_S_bb", "_Z5wHongjjPjS_S_S_bbi",
                "_Z6wSlotajjPjS_S_S_bbi", "_Z13loadFullGraphPKcPjS1_PS1_S2_S2_S2_S2_"]
 
@@ -115,6 +115,8 @@ def lib():
     L.scc_batch_run.argtypes = [vp, ctypes.c_int, u32, ctypes.c_int, vp, ctypes.POINTER(BatchResult),
                                 ctypes.POINTER(Stats)]
     L.scc_batch_destroy.argtypes = [vp]
+    L.scc_run_noalloc.argtypes = [ctypes.POINTER(CsrView), ctypes.c_int, u32, ctypes.c_int, vp,
+                                  ctypes.POINTER(Stats), vp]
     L.scc_get_trace.argtypes = [vp, ctypes.POINTER(u64), u32, ctypes.POINTER(u32), ctypes.POINTER(u64)]
     _lib = L
     return L

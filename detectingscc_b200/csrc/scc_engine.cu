@@ -471,3 +471,30 @@ extern "C" int scc_get_trace(scc_context *ctx, uint64_t *out, uint32_t cap, uint
     if (t_start) *t_start = ctx->hctl ? ctx->hctl->t_start : 0;
     return SCC_OK;
 }
+
+// Launch sequence of the single-CTA path on caller-provided scratch (used by
+// the no-allocation entry point in scc_noalloc.cu): offset validation, the
+// SCC kernel, the two canonicalisation kernels.  Allocates nothing.
+int sccb_launch_block_path(const Graph &g, const Work &w, int t1, int t2, int lw, bool hong, uint32_t *dout,
+                           cudaStream_t st, unsigned *launches)
+{
+    const size_t smem = dyn_smem_bytes(w.qcap);
+    const int vblocks = (int)std::min<uint32_t>(1184u, (g.V + 255u) / 256u + 1u);
+    k_validate<<<vblocks, 256, 0, st>>>(g, w.ctl);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_status(e);
+    void *fn = pick_block(false, hong);
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_status(e);
+    Params p{g, w, t1, t2, lw, 0u};
+    void *args[] = {&p};
+    e = cudaLaunchKernel(fn, dim3(1), dim3(BLOCK_THREADS), args, smem, st);
+    if (e != cudaSuccess) return cuda_status(e);
+    const int cb = (int)std::min<uint32_t>(1184u, (g.V + 255u) / 256u + 1u);
+    k_canon_min<<<cb, 256, 0, st>>>(w.label, w.st, g.V);
+    k_canon_write<<<cb, 256, 0, st>>>(w.label, w.st, dout, g.V);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_status(e);
+    *launches = 4;
+    return SCC_OK;
+}

@@ -133,6 +133,26 @@ const char *scc_status_string(int status);
 /* Library version string. */
 const char *scc_version(void);
 
+/* ---- run without device allocation ------------------------------------- */
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory when they need an SCC -- a process whose GPU memory is reserved up
+ * front by another allocator (a framework's caching pool, a serving process
+ * with a fixed budget), or a plugin whose host forbids allocations outside
+ * its own pool.  Runs the single-CTA SCC kernel on a scratch area that is a
+ * static __device__ array inside the library (about 1.2 MiB, held by every
+ * GPU that loads the library until the process exits); the caller passes
+ * device CSR arrays (SCC_FLAG_DEVICE is required) and a device buffer of V
+ * labels.  Graphs above SCC_NOALLOC_MAX_VERTICES / SCC_NOALLOC_MAX_EDGES
+ * are rejected with SCC_ERR_TOO_LARGE.  The first call on a device (with
+ * that device current) looks up the array's device address; make it before
+ * any stream capture.  All calls share the array: calls that overlap on the
+ * GPU race.  Calls no cudaMalloc, cudaFree or allocating library routine.
+ * Synchronous; `stream` as in scc_run. */
+#define SCC_NOALLOC_MAX_VERTICES 16384u
+#define SCC_NOALLOC_MAX_EDGES 262144u
+int scc_run_noalloc(const scc_csr_view *g, int algo, uint32_t flags, int warp_width, uint32_t *labels_out,
+                    scc_stats *stats, void *stream);
+
 /* ---- graph files ------------------------------------------------------ */
 /* A host CSR owned by the library (arrays allocated with new[], as the
  * reference loader does, load.cpp:52-115). */
