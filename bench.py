@@ -326,7 +326,43 @@ def run_reference(args):
                                    "project's iterative Tarjan oracle on one host core"},
         "e2e": {"value": v, "unit": "Medges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    ref_gpu = _reference_gpu_time(args, V, E, Fr, Fc, Br, Bc, cfg)
+    if ref_gpu:
+        out["reference_gpu"] = ref_gpu
     print(json.dumps(out), flush=True)
+
+
+def _reference_gpu_time(args, V, E, Fr, Fc, Br, Bc, cfg):
+    """The reference's own CUDA drivers (oracle/_ref/scc_ref, built from its
+    unchanged sources) on the same graph: its printed count and its own
+    "Time :" (which includes its cudaMalloc and host-to-device copies)."""
+    import re
+    import tempfile
+
+    import detectingscc_b200 as scc
+    ref = os.path.join(ROOT, "oracle", "_ref", "scc_ref")
+    if not os.path.exists(ref):
+        return None
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "graph.bin")
+        scc.save_binary(path, scc.Graph(V, E, Fr, Fc, Br, Bc))
+        runs = []
+        for _ in range(3):
+            try:
+                r = subprocess.run([ref, "-a", cfg["algo"], "-p", "1" if cfg["t1"] else "0",
+                                    "-q", "1" if cfg["t2"] else "0", "-w", str(cfg["warp"]), "-f", path],
+                                   capture_output=True, text=True, timeout=300)
+            except subprocess.TimeoutExpired:
+                return {"unavailable": "reference binary exceeded 300 s"}
+            t = re.search(r"Time : ([0-9.]+)", r.stdout)
+            n = re.search(r"Number Of Sccs : (-?\d+)", r.stdout)
+            if r.returncode != 0 or not t:
+                return {"unavailable": f"reference binary exit {r.returncode}"}
+            runs.append((float(t.group(1)), int(n.group(1)) if n else None))
+    best = min(runs)
+    return {"time_ms": best[0], "num_sccs": best[1], "Medges_per_s": round(E / (best[0] * 1e-3) / 1e6, 2),
+            "note": "reference CUDA drivers built from their sources for sm_100a; Time includes their "
+                    "cudaMalloc + H2D; best of 3"}
 
 
 def main():

@@ -101,3 +101,29 @@ def test_planted_oracle_catches_a_wrong_label(oracle_lib):
     bad[2] = 2
     assert not np.array_equal(bad, lab)
     assert lab[1:].tolist() == [1, 1, 3, 4] and n == 3
+
+
+def test_oracle_counts_match_recorded_reference_outputs(golden, oracle_lib):
+    """tests/golden/ref_counts.json holds the reference binary's own output on
+    the fixtures (recorded on a B200 by tests/golden/make_ref_counts.py)."""
+    import json
+    import os
+    from conftest import GOLDEN
+    p = os.path.join(GOLDEN, "ref_counts.json")
+    if not os.path.exists(p):
+        pytest.skip("reference outputs not recorded")
+    rec = json.load(open(p))
+    for key, r in rec.items():
+        name, algo, pp, qq, _ = key.split(":")
+        t1, t2 = int(pp[1]), int(qq[1])
+        z = golden[name]
+        V = int(z["V"])
+        Fr, Fc, Br, Bc = build_csr(V, z["src"].astype(np.int64), z["dst"].astype(np.int64))
+        fn = oracle_lib.hong if algo in "gx" else oracle_lib.slota
+        _, c = fn(V, Fr, Fc, Br, Bc, t1, t2)
+        if algo in "gx" and t2:
+            assert r["num_sccs"] <= sum(c), key       # the reference can lose a trim-2 tag
+        else:
+            assert r["num_sccs"] == sum(c), key
+        if algo == "g" and not t2:
+            assert r["numberOf1Sccs"] == c[0], key
