@@ -75,6 +75,7 @@ struct Graph {
 
 struct Work {
     uint32_t *st, *label, *stamp;
+    uint32_t *smin;             // smin[r] = smallest member id of the SCC represented by r
     uint32_t *L[2];
     uint32_t *Q[2][2];          // [direction][parity]
     uint2 *H[2][2];             // heavy chunks (vertex, chunk) [direction][parity]
@@ -361,6 +362,48 @@ __device__ __forceinline__ unsigned lbs_expand(uint32_t beg, uint32_t deg, uint3
         fn(valid, nbr, aux_o);
     }
     return total;
+}
+
+// Same walk, two entries per lane per step so that each lane has two
+// independent gathers in flight: fn(v0, n0, aux0, v1, n1, aux1).
+template <class Fn>
+__device__ __forceinline__ unsigned lbs_expand2(uint32_t beg, uint32_t deg, uint32_t aux,
+                                                const uint32_t *__restrict__ C, Fn &&fn)
+{
+    unsigned incl = warp_incl_scan(deg);
+    unsigned total = __shfl_sync(FULL, incl, 31);
+    unsigned excl = incl - deg;
+    unsigned lane = lane_id();
+    for (unsigned base = 0; base < total; base += 64u) {
+        const unsigned e0 = base + lane, e1 = e0 + 32u;
+        unsigned lo0 = 0, lo1 = 0;
+#pragma unroll
+        for (unsigned step = 16; step >= 1; step >>= 1) {
+            unsigned c0 = lo0 + step, c1 = lo1 + step;
+            unsigned x0 = __shfl_sync(FULL, excl, c0 & 31u);
+            unsigned x1 = __shfl_sync(FULL, excl, c1 & 31u);
+            if (c0 < 32u && x0 <= e0) lo0 = c0;
+            if (c1 < 32u && x1 <= e1) lo1 = c1;
+        }
+        const unsigned x0 = __shfl_sync(FULL, excl, lo0), x1 = __shfl_sync(FULL, excl, lo1);
+        const unsigned b0 = __shfl_sync(FULL, beg, lo0), b1 = __shfl_sync(FULL, beg, lo1);
+        const unsigned a0 = __shfl_sync(FULL, aux, lo0), a1 = __shfl_sync(FULL, aux, lo1);
+        const bool v0 = e0 < total, v1 = e1 < total;
+        const uint32_t n0 = v0 ? __ldg(&C[b0 + (e0 - x0)]) : 0u;
+        const uint32_t n1 = v1 ? __ldg(&C[b1 + (e1 - x1)]) : 0u;
+        fn(v0, n0, a0, v1, n1, a1);
+    }
+    return total;
+}
+
+// Fold member v into smin[rep] (the canonical label of rep's SCC): lanes
+// sharing rep reduce first, one atomicMin per group, skipped when the
+// stored value is already smaller.  All 32 lanes call.
+__device__ __forceinline__ void smin_fold(bool valid, uint32_t rep, uint32_t v, uint32_t *smin)
+{
+    unsigned grp = __match_any_sync(FULL, valid ? rep : 0xFFFFFFFFu);
+    uint32_t mn = __reduce_min_sync(grp, valid ? v : 0xFFFFFFFFu);
+    if (valid && lane_id() == (unsigned)(__ffs(grp) - 1) && mn < vld(&smin[rep])) atomicMin(&smin[rep], mn);
 }
 
 // Virtual-warp expansion: groups of W = 1 << lw lanes share one vertex and

@@ -1,9 +1,9 @@
 // Kernels and host side of the C ABI (include/scc_b200.h).
 //
-// One scc_run = (optional H2D copies) -> offset validation -> one SCC
-// launch (cooperative whole-GPU persistent kernel, or one CTA for small
-// graphs) -> two canonicalisation kernels -> (optional D2H of labels) -> one
-// D2H of the control block.  The reference instead issues one launch plus
+// One scc_run = (optional H2D copies) -> one SCC launch (cooperative
+// whole-GPU persistent kernel, or one CTA for small graphs; its first pass
+// also validates the offsets) -> one canonical-label kernel -> (optional D2H
+// of labels) -> one D2H of the control block.  The reference instead issues one launch plus
 // one or two blocking 1-byte copies per BFS level and per propagation sweep
 // (e.g. scc_WCC.cu:880-885).
 #include <cuda_runtime.h>
@@ -77,47 +77,15 @@ __global__ void __launch_bounds__(BLOCK_THREADS, 1) k_scc_block(Params p)
     if (threadIdx.x == 0) p.w.ctl->passes = ex.gl;
 }
 
-// Offsets must be the reference layout: Fr[0] = Fr[1] = 0, non-decreasing,
-// Fr[V+1] = E (load.cpp:55-77); same for Br.  Column ids are checked where
-// they are read (guard_id).
-__global__ void k_validate(Graph g, Ctl *ctl)
-{
-    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, n = gridDim.x * blockDim.x;
-    for (uint32_t i = tid; i <= g.V; i += n) {
-        if (__ldg(&g.Fr[i]) > __ldg(&g.Fr[i + 1]) || __ldg(&g.Br[i]) > __ldg(&g.Br[i + 1]))
-            set_error(ctl, E_BAD_GRAPH, 61);
-    }
-    if (tid == 0) {
-        if (g.Fr[0] != 0u || g.Fr[1] != 0u || g.Br[0] != 0u || g.Br[1] != 0u || g.Fr[g.V + 1] != g.E ||
-            g.Br[g.V + 1] != g.E)
-            set_error(ctl, E_BAD_GRAPH, 62);
-    }
-}
-
-// Canonical labels: the smallest vertex id of each representative group.
-// st[] is all DEAD (0x3FFFFFFF) once every vertex is assigned, so it serves
-// as the min-table.
-__global__ void k_canon_min(const uint32_t *__restrict__ label, uint32_t *canon, uint32_t V)
-{
-    const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t base = wid * 32u; base < V; base += nw * 32u) {
-        uint32_t v = base + lane_id() + 1u;
-        bool valid = v <= V;
-        uint32_t l = valid ? label[v] : 0xFFFFFFFFu;
-        unsigned grp = __match_any_sync(FULL, l);
-        uint32_t mn = __reduce_min_sync(grp, valid ? v : 0xFFFFFFFFu);
-        if (valid && lane_id() == (unsigned)(__ffs(grp) - 1) && l <= V && mn < canon[l]) atomicMin(&canon[l], mn);
-    }
-}
-
-__global__ void k_canon_write(const uint32_t *__restrict__ label, const uint32_t *__restrict__ canon,
+// Canonical labels: every vertex takes the smallest member id of its SCC,
+// which the update passes fold into smin[representative].
+__global__ void k_canon_write(const uint32_t *__restrict__ label, const uint32_t *__restrict__ smin,
                               uint32_t *__restrict__ out, uint32_t V)
 {
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, n = gridDim.x * blockDim.x;
     for (uint32_t v = tid + 1u; v <= V; v += n) {
         uint32_t l = label[v];
-        out[v - 1u] = l <= V ? canon[l] : 0u;
+        out[v - 1u] = l <= V ? smin[l] : 0u;
     }
 }
 
@@ -171,7 +139,7 @@ int scc_ctx_reserve(scc_context *ctx, uint32_t V, uint32_t E)
     const size_t n1 = (size_t)V + 1;
     size_t need = 0;
     auto take = [&](size_t bytes) { size_t off = need; need = align_up(need + bytes, 256); return off; };
-    size_t o_st = take(n1 * 4), o_label = take(n1 * 4), o_stamp = take(n1 * 4);
+    size_t o_st = take(n1 * 4), o_label = take(n1 * 4), o_stamp = take(n1 * 4), o_smin = take(n1 * 4);
     size_t o_L0 = take(n1 * 4), o_L1 = take(n1 * 4);
     size_t o_Q[4], o_H[4];
     for (int i = 0; i < 4; i++) o_Q[i] = take(n1 * 4);
@@ -191,6 +159,7 @@ int scc_ctx_reserve(scc_context *ctx, uint32_t V, uint32_t E)
     w.st = (uint32_t *)(b + o_st);
     w.label = (uint32_t *)(b + o_label);
     w.stamp = (uint32_t *)(b + o_stamp);
+    w.smin = (uint32_t *)(b + o_smin);
     w.L[0] = (uint32_t *)(b + o_L0);
     w.L[1] = (uint32_t *)(b + o_L1);
     w.Q[0][0] = (uint32_t *)(b + o_Q[0]);
@@ -365,10 +334,6 @@ extern "C" int scc_run(scc_context *ctx, const scc_csr_view *gv, int algo, uint3
     CK(cudaMemcpyAsync(ctx->work.ctl, ctx->hctl, sizeof(Ctl), cudaMemcpyHostToDevice, st));
     CK(cudaMemsetAsync(ctx->work.pivkey, 0, hong ? (4 * ((size_t)V + 1) + 8) * 8 : 8, st));
 
-    const int vblocks = std::min<int>(ctx->nsm * 4, (int)((V + 255) / 256) + 1);
-    k_validate<<<vblocks, 256, 0, st>>>(g, ctx->work.ctl);
-    launches++;
-    CK(cudaGetLastError());
 
     ctx->work.qcap = ctx->qcap;
     ctx->work.bu_den = ctx->bu_den;
@@ -397,9 +362,8 @@ extern "C" int scc_run(scc_context *ctx, const scc_csr_view *gv, int algo, uint3
     CK(cudaEventRecord(ctx->ev[2], st));
     if (dout) {
         const int cb = std::min<int>(ctx->nsm * 8, (int)((V + 255) / 256) + 1);
-        k_canon_min<<<cb, 256, 0, st>>>(ctx->work.label, ctx->work.st, V);
-        k_canon_write<<<cb, 256, 0, st>>>(ctx->work.label, ctx->work.st, dout, V);
-        launches += 2;
+        k_canon_write<<<cb, 256, 0, st>>>(ctx->work.label, ctx->work.smin, dout, V);
+        launches += 1;
         CK(cudaGetLastError());
         if (!dev) CK(cudaMemcpyAsync(labels_out, dout, (size_t)V * 4, cudaMemcpyDeviceToHost, st));
     }
@@ -473,28 +437,24 @@ extern "C" int scc_get_trace(scc_context *ctx, uint64_t *out, uint32_t cap, uint
 }
 
 // Launch sequence of the single-CTA path on caller-provided scratch (used by
-// the no-allocation entry point in scc_noalloc.cu): offset validation, the
-// SCC kernel, the two canonicalisation kernels.  Allocates nothing.
+// the no-allocation entry point in scc_noalloc.cu): the SCC kernel (which
+// also validates the offsets) and the canonical-label kernel.  Allocates
+// nothing.
 int sccb_launch_block_path(const Graph &g, const Work &w, int t1, int t2, int lw, bool hong, uint32_t *dout,
                            cudaStream_t st, unsigned *launches)
 {
     const size_t smem = dyn_smem_bytes(w.qcap);
-    const int vblocks = (int)std::min<uint32_t>(1184u, (g.V + 255u) / 256u + 1u);
-    k_validate<<<vblocks, 256, 0, st>>>(g, w.ctl);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_status(e);
     void *fn = pick_block(false, hong);
-    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return cuda_status(e);
     Params p{g, w, t1, t2, lw, 0u};
     void *args[] = {&p};
     e = cudaLaunchKernel(fn, dim3(1), dim3(BLOCK_THREADS), args, smem, st);
     if (e != cudaSuccess) return cuda_status(e);
     const int cb = (int)std::min<uint32_t>(1184u, (g.V + 255u) / 256u + 1u);
-    k_canon_min<<<cb, 256, 0, st>>>(w.label, w.st, g.V);
-    k_canon_write<<<cb, 256, 0, st>>>(w.label, w.st, dout, g.V);
+    k_canon_write<<<cb, 256, 0, st>>>(w.label, w.smin, dout, g.V);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_status(e);
-    *launches = 4;
+    *launches = 2;
     return SCC_OK;
 }

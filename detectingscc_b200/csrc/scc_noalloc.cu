@@ -48,7 +48,7 @@ constexpr size_t al256(size_t x) { return (x + 255) / 256 * 256; }
 // table and the control block).
 constexpr size_t scratch_bytes(size_t V, size_t E)
 {
-    return al256((V + 1) * 4) * 9 + al256((E / CH + E / HEAVY_T + 64) * 8) * 4 + al256((4 * (V + 1) + 8) * 8) +
+    return al256((V + 1) * 4) * 10 + al256((E / CH + E / HEAVY_T + 64) * 8) * 4 + al256((4 * (V + 1) + 8) * 8) +
            al256(sizeof(Ctl));
 }
 
@@ -132,6 +132,7 @@ extern "C" int scc_run_noalloc(const scc_csr_view *gv, int algo, uint32_t flags,
     w.st = (uint32_t *)take(n1 * 4);
     w.label = (uint32_t *)take(n1 * 4);
     w.stamp = (uint32_t *)take(n1 * 4);
+    w.smin = (uint32_t *)take(n1 * 4);
     w.L[0] = (uint32_t *)take(n1 * 4);
     w.L[1] = (uint32_t *)take(n1 * 4);
     w.Q[0][0] = (uint32_t *)take(n1 * 4);
@@ -146,7 +147,7 @@ extern "C" int scc_run_noalloc(const scc_csr_view *gv, int algo, uint32_t flags,
     w.pivkey = (unsigned long long *)take((4 * n1 + 8) * 8);
     w.ctl = (Ctl *)take(sizeof(Ctl));
     w.qcap = NOALLOC_QCAP;
-    w.bu_den = 16;
+    w.bu_den = 32;
     if (off > NOALLOC_BYTES) return SCC_ERR_TOO_LARGE;
 
     cudaStream_t st = (cudaStream_t)stream;

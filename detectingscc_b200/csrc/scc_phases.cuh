@@ -99,11 +99,20 @@ __device__ __forceinline__ uint32_t trim2_partner(const Graph &g, const uint32_t
 template <class Ex>
 __device__ bool ph_init(Ex &ex, const Graph &g, const Work &w, bool fold_pivot)
 {
+    // Also checks the offsets (the reference layout: Fr[0] = Fr[1] = 0,
+    // non-decreasing, Fr[V+1] = E, load.cpp:55-77; same for Br).  A bad
+    // graph sets the error before the barrier, so no later pass runs.
     return run_pass(ex, PH_INIT, [&](unsigned, unsigned) {
         unsigned long long best = 0;
+        if (ex.leader() && (g.Fr[0] != 0u || g.Fr[1] != 0u || g.Br[0] != 0u || g.Br[1] != 0u ||
+                            g.Fr[g.V + 1] != g.E || g.Br[g.V + 1] != g.E))
+            set_error(ex.ctl, E_BAD_GRAPH, 62);
         for (uint32_t i = ex.tid(); i <= g.V; i += ex.nthr()) {
+            if (__ldg(&g.Fr[i]) > __ldg(&g.Fr[i + 1]) || __ldg(&g.Br[i]) > __ldg(&g.Br[i + 1]))
+                set_error(ex.ctl, E_BAD_GRAPH, 61);
             w.st[i] = (i == 0u) ? DEAD : 0u;
             w.stamp[i] = 0u;
+            w.smin[i] = DEAD;
             if (fold_pivot && i != 0u) {
                 unsigned long long k = pivot_key(g, i);
                 best = k > best ? k : best;
@@ -138,6 +147,7 @@ __device__ bool ph_trim1_once(Ex &ex, const Graph &g, const Work &w, uint32_t *L
                 if (indeg == 0u || outdeg == 0u) {
                     w.st[v] = DEAD;
                     w.label[v] = v;
+                    w.smin[v] = v;
                     ntrim++;
                 } else {
                     surv = true;
@@ -185,7 +195,7 @@ __device__ bool ph_trim1_fix(Ex &ex, const Graph &g, const Work &w, VList src0, 
                         else
                             trim = !has_live(ex, w.st, g.Br, g.Bc, v, r, g.V) ||
                                    !has_live(ex, w.st, g.Fr, g.Fc, v, r, g.V);
-                        if (trim) { w.st[v] = DEAD; w.label[v] = v; }
+                        if (trim) { w.st[v] = DEAD; w.label[v] = v; w.smin[v] = v; }
                     }
                 }
                 count_verts(ex, valid);
@@ -243,6 +253,7 @@ __device__ bool ph_trim2(Ex &ex, const Graph &g, const Work &w, VList src)
                         hit = true;
                         cnt = v <= k;
                         w.label[v] = v < k ? v : k;
+                        if (v <= k) w.smin[v] = v;
                     }
                 }
             }
@@ -284,6 +295,26 @@ __device__ __forceinline__ void bfs_edge_visit(Ex &ex, const Graph &g, const Wor
     bq_push((unsigned)dir, claim, nbr, w.qcap, w.Q[dir][par], &ex.ctl->lc[nxt][C_FQ + dir], g.V, ex.ctl, 13);
 }
 
+// Two adjacency entries per lane: both gathers and both claims are issued
+// before either append, so every lane keeps two requests in flight.
+template <class Ex>
+__device__ __forceinline__ void bfs_edge_visit2(Ex &ex, const Graph &g, const Work &w, int dir, bool v0, uint32_t n0,
+                                                uint32_t r0, bool v1, uint32_t n1, uint32_t r1, unsigned par,
+                                                unsigned nxt)
+{
+    const uint32_t bit = dir ? BVB : FVB;
+    if (v0) n0 = guard_id(n0, g.V, ex.ctl);
+    if (v1) n1 = guard_id(n1, g.V, ex.ctl);
+    const uint32_t s0 = v0 ? w.st[n0] : DEAD;
+    const uint32_t s1 = v1 ? w.st[n1] : DEAD;
+    const bool t0 = v0 && (s0 & (RMASK | bit)) == r0;
+    const bool t1 = v1 && (s1 & (RMASK | bit)) == r1;
+    const uint32_t o0 = t0 ? atomicOr(&w.st[n0], bit) : bit;
+    const uint32_t o1 = t1 ? atomicOr(&w.st[n1], bit) : bit;
+    bq_push((unsigned)dir, !(o0 & bit), n0, w.qcap, w.Q[dir][par], &ex.ctl->lc[nxt][C_FQ + dir], g.V, ex.ctl, 13);
+    bq_push((unsigned)dir, !(o1 & bit), n1, w.qcap, w.Q[dir][par], &ex.ctl->lc[nxt][C_FQ + dir], g.V, ex.ctl, 13);
+}
+
 template <class Ex>
 __device__ __forceinline__ void bfs_expand_lanes(Ex &ex, const Graph &g, const Work &w, int dir, uint32_t v,
                                                  bool act, uint32_t r, int lw, unsigned par, unsigned nxt)
@@ -297,8 +328,16 @@ __device__ __forceinline__ void bfs_expand_lanes(Ex &ex, const Graph &g, const W
     if (lw > 0 && (lane_id() & ((1u << lw) - 1u)) != 0u) nch = 0u;
     warp_push_chunks(v, nch, w.H[dir][par], &ex.ctl->lc[nxt][C_FH + dir], w.hcap, ex.ctl);
     if (heavy) deg = 0u;
-    auto fn = [&](bool valid, uint32_t nbr, uint32_t rr) { bfs_edge_visit(ex, g, w, dir, valid, nbr, rr, par, nxt); };
-    unsigned tot = (lw < 0) ? lbs_expand(beg, deg, r, C, fn) : vw_expand(beg, deg, r, (unsigned)lw, C, fn);
+    unsigned tot;
+    if (lw < 0) {
+        auto fn2 = [&](bool v0, uint32_t n0, uint32_t r0, bool v1, uint32_t n1, uint32_t r1) {
+            bfs_edge_visit2(ex, g, w, dir, v0, n0, r0, v1, n1, r1, par, nxt);
+        };
+        tot = lbs_expand2(beg, deg, r, C, fn2);
+    } else {
+        auto fn = [&](bool valid, uint32_t nbr, uint32_t rr) { bfs_edge_visit(ex, g, w, dir, valid, nbr, rr, par, nxt); };
+        tot = vw_expand(beg, deg, r, (unsigned)lw, C, fn);
+    }
     count_edges(ex, tot);
 }
 
@@ -309,11 +348,12 @@ __device__ __forceinline__ void chunk_expand(Ex &ex, const uint32_t *__restrict_
 {
     uint32_t beg = __ldg(&R[hc.x]) + hc.y * CH;
     uint32_t end = min(__ldg(&R[hc.x + 1]), beg + CH);
-    for (uint32_t k = lane_id(); k < CH; k += 32u) {
-        uint32_t e = beg + k;
-        bool valid = e < end;
-        uint32_t nbr = valid ? __ldg(&C[e]) : 0u;
-        fn(valid, nbr, aux);
+    for (uint32_t k = lane_id(); k < CH; k += 64u) {
+        const uint32_t e0 = beg + k, e1 = e0 + 32u;
+        const bool v0 = e0 < end, v1 = e1 < end;
+        const uint32_t n0 = v0 ? __ldg(&C[e0]) : 0u;
+        const uint32_t n1 = v1 ? __ldg(&C[e1]) : 0u;
+        fn(v0, n0, aux, v1, n1, aux);
     }
     count_edges(ex, end > beg ? end - beg : 0u);
 }
@@ -418,8 +458,10 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
             for (uint32_t c = ex.wid(); c < nfc + nbc; c += ex.nwarps()) {
                 const int dir = c < nfc ? 0 : 1;
                 const uint2 hc = make_uint2(p, dir ? c - nfc : c);
-                auto fn = [&](bool valid, uint32_t nbr, uint32_t rr) { bfs_edge_visit(ex, g, w, dir, valid, nbr, rr, par, nxt); };
-                chunk_expand(ex, dir ? g.Br : g.Fr, dir ? g.Bc : g.Fc, hc, r, fn);
+                auto fn2 = [&](bool v0, uint32_t n0, uint32_t r0, bool v1, uint32_t n1, uint32_t r1) {
+                    bfs_edge_visit2(ex, g, w, dir, v0, n0, r0, v1, n1, r1, par, nxt);
+                };
+                chunk_expand(ex, dir ? g.Br : g.Fr, dir ? g.Bc : g.Fc, hc, r, fn2);
             }
         }
         for (uint32_t it = ex.wid(); it < ng; it += ex.nwarps()) {
@@ -465,8 +507,10 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
                 if (k < nh) {
                     uint2 hc = w.H[dir][cp][k];
                     uint32_t r = w.st[hc.x] & RMASK;
-                    auto fn = [&](bool valid, uint32_t nbr, uint32_t rr) { bfs_edge_visit(ex, g, w, dir, valid, nbr, rr, par, nxt); };
-                    chunk_expand(ex, dir ? g.Br : g.Fr, dir ? g.Bc : g.Fc, hc, r, fn);
+                    auto fn2 = [&](bool v0, uint32_t n0, uint32_t r0, bool v1, uint32_t n1, uint32_t r1) {
+                        bfs_edge_visit2(ex, g, w, dir, v0, n0, r0, v1, n1, r1, par, nxt);
+                    };
+                    chunk_expand(ex, dir ? g.Br : g.Fr, dir ? g.Bc : g.Fc, hc, r, fn2);
                 } else {
                     const uint32_t gi = k - nh;
                     const uint32_t n = dir ? nb : nf;
@@ -527,10 +571,14 @@ __device__ bool ph_propagate(Ex &ex, const Graph &g, const Work &w, VList src0)
             const uint32_t hn = first ? 0u : nh;
             const uint32_t ng = (src.n + 31u) / 32u;
             auto fn = [&](bool valid, uint32_t u, uint32_t c) { prop_visit<MAXP>(ex, g, w, valid, u, c, par, nxt, tag); };
+            auto fn2 = [&](bool v0, uint32_t u0, uint32_t c0, bool v1, uint32_t u1, uint32_t c1) {
+                prop_visit<MAXP>(ex, g, w, v0, u0, c0, par, nxt, tag);
+                prop_visit<MAXP>(ex, g, w, v1, u1, c1, par, nxt, tag);
+            };
             for (uint32_t it = ex.wid(); it < hn + ng; it += ex.nwarps()) {
                 if (it < hn) {
                     uint2 hc = w.H[0][cp][it];
-                    chunk_expand(ex, g.Br, g.Bc, hc, w.st[hc.x] & RMASK, fn);
+                    chunk_expand(ex, g.Br, g.Bc, hc, w.st[hc.x] & RMASK, fn2);
                 } else {
                     uint32_t i = (it - hn) * 32u + lane_id();
                     bool valid = i < src.n;
@@ -572,13 +620,16 @@ __device__ bool ph_hong_update(Ex &ex, const Graph &g, const Work &w, VList src,
             uint32_t i = base + lane_id();
             bool valid = i < src.n, surv = false;
             uint32_t v = valid ? src.at(i) : 0u, nr = 0u;
+            uint32_t p = 0u;
+            bool scc = false;
             if (valid) {
                 uint32_t s = w.st[v];
                 if (s != DEAD) {
-                    uint32_t p = key_vertex(w.pivkey[single ? 0u : (s & RMASK)]);
+                    p = key_vertex(w.pivkey[single ? 0u : (s & RMASK)]);
                     if ((s & FVB) && (s & BVB)) {
                         w.st[v] = DEAD;
                         w.label[v] = p;
+                        scc = true;
                     } else {
                         nr = split_name(g.V, p, s);
                         w.st[v] = nr;
@@ -587,6 +638,7 @@ __device__ bool ph_hong_update(Ex &ex, const Graph &g, const Work &w, VList src,
                 }
             }
             count_verts(ex, valid);
+            smin_fold(scc, p, v, w.smin);
             bq_push(0, surv, v, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 15);
             if (fold) range_max_atomic(surv, nr, surv ? pivot_key(g, v) : 0ull, w.pivkey);
         }
@@ -606,14 +658,16 @@ __device__ bool ph_slota_first_update(Ex &ex, const Graph &g, const Work &w, VLi
             uint32_t i = base + lane_id();
             bool valid = i < src.n, surv = false;
             uint32_t v = valid ? src.at(i) : 0u;
+            bool scc = false;
             if (valid) {
                 uint32_t s = w.st[v];
                 if (s != DEAD) {
-                    if ((s & FVB) && (s & BVB)) { w.st[v] = DEAD; w.label[v] = p; }
+                    if ((s & FVB) && (s & BVB)) { w.st[v] = DEAD; w.label[v] = p; scc = true; }
                     else { w.st[v] = v; surv = true; }
                 }
             }
             count_verts(ex, valid);
+            smin_fold(scc, p, v, w.smin);
             bq_push(0, surv, v, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 16);
         }
         bq_flush(1, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], nullptr, nullptr, g.V, ex.ctl);
@@ -631,12 +685,15 @@ __device__ bool ph_slota_peel_update(Ex &ex, const Graph &g, const Work &w, VLis
             uint32_t i = base + lane_id();
             bool valid = i < src.n, surv = false;
             uint32_t v = valid ? src.at(i) : 0u;
+            bool scc = false;
+            uint32_t c = 0u;
             if (valid) {
                 uint32_t s = w.st[v];
-                if (s & FVB) { w.st[v] = DEAD; w.label[v] = s & RMASK; }
+                if (s & FVB) { c = s & RMASK; w.st[v] = DEAD; w.label[v] = c; scc = true; }
                 else { w.st[v] = v; surv = true; }
             }
             count_verts(ex, valid);
+            smin_fold(scc, c, v, w.smin);
             bq_push(0, surv, v, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 17);
         }
         bq_flush(1, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], nullptr, nullptr, g.V, ex.ctl);
