@@ -41,7 +41,7 @@ constexpr int E_NOT_CONVERGED = 21;
 constexpr int E_TIMEOUT = 22;
 constexpr int E_BAD_GRAPH = 23;
 
-enum { C_FQ = 0, C_BQ = 1, C_FH = 2, C_BH = 3, C_LIST = 4, C_AUX = 5, NCNT = 8 };
+enum { C_FQ = 0, C_BQ = 1, C_FH = 2, C_BH = 3, C_LIST = 4, C_FE = 5, C_BE = 6, NCNT = 8 };
 
 struct __align__(128) Ctl {
     // grid barrier arrival counter and the sticky error code share one
@@ -71,7 +71,24 @@ enum {
 struct Graph {
     uint32_t V, E;
     const uint32_t *__restrict__ Fr, *__restrict__ Fc, *__restrict__ Br, *__restrict__ Bc;
+    uint32_t vec;   // Fr and Br are 16-byte aligned: 128-bit offset loads allowed
 };
+
+// o[0..4] = R[i0 .. i0+4] with indices clipped to V+1 (the last offset);
+// one 128-bit load plus one 32-bit load when R is 16-byte aligned (i0 is a
+// multiple of 4).
+__device__ __forceinline__ void load_off5(const uint32_t *__restrict__ R, uint32_t i0, uint32_t V, uint32_t vec,
+                                          uint32_t (&o)[5])
+{
+    if (vec && i0 + 4u <= V + 1u) {
+        const uint4 x = __ldg(reinterpret_cast<const uint4 *>(R + i0));
+        o[0] = x.x; o[1] = x.y; o[2] = x.z; o[3] = x.w;
+        o[4] = __ldg(&R[i0 + 4u]);
+    } else {
+#pragma unroll
+        for (int j = 0; j < 5; j++) o[j] = __ldg(&R[min(i0 + (uint32_t)j, V + 1u)]);
+    }
+}
 
 struct Work {
     uint32_t *st, *label, *stamp;
@@ -83,7 +100,7 @@ struct Work {
     unsigned long long *pivkey; // Hong: 4V+4 slots; Slota: 1
     Ctl *ctl;
     uint32_t qcap;              // entries per CTA staging queue (dynamic shared memory)
-    uint32_t bu_den;            // bottom-up BFS when frontier > scope / bu_den (0 = never)
+    uint32_t bu_k;              // bottom-up BFS step when frontier edges > bu_k * scope vertices (0 = never)
 };
 
 // Dynamic shared memory of the SCC kernels: 16 control words, then NBQ
@@ -274,9 +291,18 @@ __device__ __forceinline__ void bq_push(unsigned qi, bool pred, uint32_t val, ui
     warp_push(spill, val, gq, gcnt, gcap, ctl, where);
 }
 
-// Called by every thread of the CTA at the end of a pass.
+// Adds x to the CTA's frontier-edge tally of queue qi (words 12, 13).
+__device__ __forceinline__ void bq_add_edges(unsigned qi, unsigned x)
+{
+    x = __reduce_add_sync(FULL, x);
+    if (lane_id() == 0 && x) atomicAdd(&sccb_dsmem[12 + qi], x);
+}
+
+// Called by every thread of the CTA at the end of a pass.  ecnt0 / ecnt1
+// (optional) receive the CTA's frontier-edge tallies.
 __device__ __forceinline__ void bq_flush(unsigned nq, uint32_t qcap, uint32_t *gq0, unsigned *gcnt0, uint32_t *gq1,
-                                         unsigned *gcnt1, uint32_t gcap, Ctl *ctl)
+                                         unsigned *gcnt1, uint32_t gcap, Ctl *ctl, unsigned *ecnt0 = nullptr,
+                                         unsigned *ecnt1 = nullptr)
 {
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -285,6 +311,9 @@ __device__ __forceinline__ void bq_flush(unsigned nq, uint32_t qcap, uint32_t *g
             sccb_dsmem[4 + qi] = n;
             sccb_dsmem[8 + qi] = n ? atomicAdd(qi ? gcnt1 : gcnt0, n) : 0u;
             sccb_dsmem[qi] = 0u;
+            unsigned *ec = qi ? ecnt1 : ecnt0;
+            if (ec && sccb_dsmem[12 + qi]) atomicAdd(ec, sccb_dsmem[12 + qi]);
+            sccb_dsmem[12 + qi] = 0u;
         }
     }
     __syncthreads();
@@ -401,6 +430,7 @@ __device__ __forceinline__ unsigned lbs_expand2(uint32_t beg, uint32_t deg, uint
 // stored value is already smaller.  All 32 lanes call.
 __device__ __forceinline__ void smin_fold(bool valid, uint32_t rep, uint32_t v, uint32_t *smin)
 {
+    if (__ballot_sync(FULL, valid) == 0u) return;
     unsigned grp = __match_any_sync(FULL, valid ? rep : 0xFFFFFFFFu);
     uint32_t mn = __reduce_min_sync(grp, valid ? v : 0xFFFFFFFFu);
     if (valid && lane_id() == (unsigned)(__ffs(grp) - 1) && mn < vld(&smin[rep])) atomicMin(&smin[rep], mn);

@@ -310,7 +310,7 @@ extern "C" int scc_run(scc_context *ctx, const scc_csr_view *gv, int algo, uint3
     unsigned launches = 0;
 
     CK(cudaEventRecord(ctx->ev[0], st));
-    Graph g{V, E, gv->Fr, gv->Fc, gv->Br, gv->Bc};
+    Graph g{V, E, gv->Fr, gv->Fc, gv->Br, gv->Bc, 0u};
     uint32_t *dout = labels_out;
     if (!dev) {
         rc = ensure_csr_mirror(ctx, V, E);
@@ -325,6 +325,7 @@ extern "C" int scc_run(scc_context *ctx, const scc_csr_view *gv, int algo, uint3
         dout = labels_out ? ctx->dlab : nullptr;
     }
     if (!E) { g.Fc = g.Fc ? g.Fc : ctx->work.st; g.Bc = g.Bc ? g.Bc : ctx->work.st; }
+    g.vec = ((((uintptr_t)g.Fr) | ((uintptr_t)g.Br)) & 15u) == 0u ? 1u : 0u;
 
     // control block: zeroed, then the timeout
     memset(ctx->hctl, 0, sizeof(Ctl));
@@ -336,7 +337,7 @@ extern "C" int scc_run(scc_context *ctx, const scc_csr_view *gv, int algo, uint3
 
 
     ctx->work.qcap = ctx->qcap;
-    ctx->work.bu_den = ctx->bu_den;
+    ctx->work.bu_k = ctx->bu_k;
     const size_t smem = dyn_smem_bytes(ctx->qcap);
     Params p{g, ctx->work, (flags & SCC_FLAG_TRIM1) ? 1 : 0, (flags & SCC_FLAG_TRIM2) ? 1 : 0, lw, ctx->tail_vertices};
     bool use_block = (V <= ctx->block_max_vertices && E <= ctx->block_max_edges);
@@ -401,7 +402,7 @@ extern "C" int scc_set_tuning(scc_context *ctx, const char *key, long long value
     else if (!strcmp(key, "block_max_edges")) ctx->block_max_edges = (uint32_t)value;
     else if (!strcmp(key, "timeout_ms")) ctx->timeout_ms = (uint32_t)value;
     else if (!strcmp(key, "max_blocks_per_sm")) ctx->max_blocks_per_sm = (int)value;
-    else if (!strcmp(key, "bu_den")) ctx->bu_den = (uint32_t)value;
+    else if (!strcmp(key, "bu_k")) ctx->bu_k = (uint32_t)value;
     else if (!strcmp(key, "qcap")) {
         if (value < 256 || value > 24576) return SCC_ERR_INVALID_ARG;
         ctx->qcap = (uint32_t)value;

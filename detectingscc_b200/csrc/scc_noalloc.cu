@@ -147,11 +147,12 @@ extern "C" int scc_run_noalloc(const scc_csr_view *gv, int algo, uint32_t flags,
     w.pivkey = (unsigned long long *)take((4 * n1 + 8) * 8);
     w.ctl = (Ctl *)take(sizeof(Ctl));
     w.qcap = NOALLOC_QCAP;
-    w.bu_den = 32;
+    w.bu_k = 1;
     if (off > NOALLOC_BYTES) return SCC_ERR_TOO_LARGE;
 
     cudaStream_t st = (cudaStream_t)stream;
-    Graph g{V, E, gv->Fr, gv->Fc ? gv->Fc : w.st, gv->Br, gv->Bc ? gv->Bc : w.st};
+    Graph g{V, E, gv->Fr, gv->Fc ? gv->Fc : w.st, gv->Br, gv->Bc ? gv->Bc : w.st,
+            ((((uintptr_t)gv->Fr) | ((uintptr_t)gv->Br)) & 15u) == 0u ? 1u : 0u};
     k_noalloc_ctl_init<<<1, 32, 0, st>>>(w.ctl, 4000ull * 1000000ull);
     if (cudaMemsetAsync(w.pivkey, 0, hong ? (4 * n1 + 8) * 8 : 8, st) != cudaSuccess) {
         cudaGetLastError();

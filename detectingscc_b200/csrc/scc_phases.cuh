@@ -17,6 +17,23 @@ struct VList {
     __device__ __forceinline__ uint32_t at(uint32_t i) const { return p ? p[i] : base + i; }
 };
 
+// Four consecutive entries of a list for this lane (entries i0 .. i0+3): one
+// 128-bit load for explicit lists (list buffers are 256-byte aligned).
+__device__ __forceinline__ void load_list4(const VList &src, uint32_t i0, uint32_t (&v)[4], bool (&ok)[4])
+{
+    if (src.p && i0 + 3u < src.n) {
+        const uint4 x = *reinterpret_cast<const uint4 *>(src.p + i0);
+        v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+        ok[0] = ok[1] = ok[2] = ok[3] = true;
+        return;
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        ok[j] = i0 + (uint32_t)j < src.n;
+        v[j] = ok[j] ? src.at(i0 + (uint32_t)j) : 0u;
+    }
+}
+
 template <class Ex>
 __device__ __forceinline__ void count_edges(Ex &ex, unsigned warp_total)
 {
@@ -30,6 +47,14 @@ __device__ __forceinline__ void count_verts(Ex &ex, bool valid)
     if constexpr (Ex::instr) {
         unsigned m = __ballot_sync(FULL, valid);
         if (lane_id() == 0 && m) atomicAdd(&ex.ctl->t_verts, (unsigned long long)__popc(m));
+    }
+}
+template <class Ex>
+__device__ __forceinline__ void count_verts_n(Ex &ex, unsigned n)
+{
+    if constexpr (Ex::instr) {
+        n = __reduce_add_sync(FULL, n);
+        if (lane_id() == 0 && n) atomicAdd(&ex.ctl->t_verts, (unsigned long long)n);
     }
 }
 
@@ -102,22 +127,42 @@ __device__ bool ph_init(Ex &ex, const Graph &g, const Work &w, bool fold_pivot)
     // Also checks the offsets (the reference layout: Fr[0] = Fr[1] = 0,
     // non-decreasing, Fr[V+1] = E, load.cpp:55-77; same for Br).  A bad
     // graph sets the error before the barrier, so no later pass runs.
+    // Four ids per lane: 128-bit offset loads and state stores.
     return run_pass(ex, PH_INIT, [&](unsigned, unsigned) {
         unsigned long long best = 0;
         if (ex.leader() && (g.Fr[0] != 0u || g.Fr[1] != 0u || g.Br[0] != 0u || g.Br[1] != 0u ||
                             g.Fr[g.V + 1] != g.E || g.Br[g.V + 1] != g.E))
             set_error(ex.ctl, E_BAD_GRAPH, 62);
-        for (uint32_t i = ex.tid(); i <= g.V; i += ex.nthr()) {
-            if (__ldg(&g.Fr[i]) > __ldg(&g.Fr[i + 1]) || __ldg(&g.Br[i]) > __ldg(&g.Br[i + 1]))
-                set_error(ex.ctl, E_BAD_GRAPH, 61);
-            w.st[i] = (i == 0u) ? DEAD : 0u;
-            w.stamp[i] = 0u;
-            w.smin[i] = DEAD;
-            if (fold_pivot && i != 0u) {
-                unsigned long long k = pivot_key(g, i);
-                best = k > best ? k : best;
+        bool bad = false;
+        for (uint32_t i0 = ex.tid() * 4u; i0 <= g.V; i0 += ex.nthr() * 4u) {
+            uint32_t f[5], b[5];
+            load_off5(g.Fr, i0, g.V, g.vec, f);
+            load_off5(g.Br, i0, g.V, g.vec, b);
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const uint32_t i = i0 + (uint32_t)j;
+                if (i <= g.V) {
+                    bad |= f[j] > f[j + 1] || b[j] > b[j + 1];
+                    if (fold_pivot && i != 0u) {
+                        unsigned long long k = ((unsigned long long)((f[j + 1] - f[j]) * (b[j + 1] - b[j])) << 32) |
+                                               (0xFFFFFFFFu - i);
+                        best = k > best ? k : best;
+                    }
+                }
+            }
+            if (i0 + 3u <= g.V) {
+                *reinterpret_cast<uint4 *>(w.st + i0) = make_uint4(i0 == 0u ? DEAD : 0u, 0u, 0u, 0u);
+                *reinterpret_cast<uint4 *>(w.stamp + i0) = make_uint4(0u, 0u, 0u, 0u);
+                *reinterpret_cast<uint4 *>(w.smin + i0) = make_uint4(DEAD, DEAD, DEAD, DEAD);
+            } else {
+                for (uint32_t i = i0; i <= g.V; i++) {
+                    w.st[i] = (i == 0u) ? DEAD : 0u;
+                    w.stamp[i] = 0u;
+                    w.smin[i] = DEAD;
+                }
             }
         }
+        if (bad) set_error(ex.ctl, E_BAD_GRAPH, 61);
         if (fold_pivot) block_max_atomic(best, &w.pivkey[0]);
     });
 }
@@ -134,29 +179,41 @@ __device__ bool ph_trim1_once(Ex &ex, const Graph &g, const Work &w, uint32_t *L
     // then has a live same-range in-neighbour iff its in-degree is non-zero
     // (self-loops count, as in trim1), so the decision reads the offsets
     // only and the pass can mark vertices as it goes.  Survivors are
-    // compacted into Lout and bid for the first pivot.
+    // compacted into Lout and bid for the first pivot.  Four ids per lane.
     return run_pass(ex, PH_TRIM1_ONCE, [&](unsigned, unsigned nxt) {
         unsigned long long best = 0;
         unsigned ntrim = 0;
-        for (uint32_t base = ex.wid() * 32u; base < g.V; base += ex.nwarps() * 32u) {
-            uint32_t v = base + lane_id() + 1u;
-            bool valid = v <= g.V, surv = false;
-            if (valid) {
-                const uint32_t indeg = __ldg(&g.Br[v + 1]) - __ldg(&g.Br[v]);
-                const uint32_t outdeg = __ldg(&g.Fr[v + 1]) - __ldg(&g.Fr[v]);
-                if (indeg == 0u || outdeg == 0u) {
-                    w.st[v] = DEAD;
-                    w.label[v] = v;
-                    w.smin[v] = v;
-                    ntrim++;
-                } else {
-                    surv = true;
-                    unsigned long long k = ((unsigned long long)(outdeg * indeg) << 32) | (0xFFFFFFFFu - v);
-                    best = k > best ? k : best;
-                }
+        for (uint32_t base = ex.wid() * 128u; base <= g.V; base += ex.nwarps() * 128u) {
+            const uint32_t i0 = base + 4u * lane_id();
+            uint32_t f[5], b[5];
+            if (i0 <= g.V) {
+                load_off5(g.Fr, i0, g.V, g.vec, f);
+                load_off5(g.Br, i0, g.V, g.vec, b);
+            } else {
+#pragma unroll
+                for (int j = 0; j < 5; j++) f[j] = b[j] = 0u;
             }
-            count_verts(ex, valid);
-            bq_push(0, surv, v, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 10);
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const uint32_t v = i0 + (uint32_t)j;
+                const bool valid = v >= 1u && v <= g.V;
+                bool surv = false;
+                if (valid) {
+                    const uint32_t indeg = b[j + 1] - b[j], outdeg = f[j + 1] - f[j];
+                    if (indeg == 0u || outdeg == 0u) {
+                        w.st[v] = DEAD;
+                        w.label[v] = v;
+                        w.smin[v] = v;
+                        ntrim++;
+                    } else {
+                        surv = true;
+                        unsigned long long k = ((unsigned long long)(outdeg * indeg) << 32) | (0xFFFFFFFFu - v);
+                        best = k > best ? k : best;
+                    }
+                }
+                bq_push(0, surv, v, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 10);
+            }
+            count_verts_n(ex, i0 <= g.V ? min(4u, g.V + 1u - i0) : 0u);
         }
         ntrim = __reduce_add_sync(FULL, ntrim);
         if (lane_id() == 0 && ntrim) atomicAdd(&ex.ctl->n_trim1, (unsigned long long)ntrim);
@@ -292,6 +349,8 @@ __device__ __forceinline__ void bfs_edge_visit(Ex &ex, const Graph &g, const Wor
         uint32_t s = w.st[nbr];
         if ((s & (RMASK | bit)) == r) claim = !(atomicOr(&w.st[nbr], bit) & bit);
     }
+    const uint32_t *Rn = dir ? g.Br : g.Fr;
+    bq_add_edges((unsigned)dir, claim ? __ldg(&Rn[nbr + 1]) - __ldg(&Rn[nbr]) : 0u);
     bq_push((unsigned)dir, claim, nbr, w.qcap, w.Q[dir][par], &ex.ctl->lc[nxt][C_FQ + dir], g.V, ex.ctl, 13);
 }
 
@@ -311,8 +370,15 @@ __device__ __forceinline__ void bfs_edge_visit2(Ex &ex, const Graph &g, const Wo
     const bool t1 = v1 && (s1 & (RMASK | bit)) == r1;
     const uint32_t o0 = t0 ? atomicOr(&w.st[n0], bit) : bit;
     const uint32_t o1 = t1 ? atomicOr(&w.st[n1], bit) : bit;
-    bq_push((unsigned)dir, !(o0 & bit), n0, w.qcap, w.Q[dir][par], &ex.ctl->lc[nxt][C_FQ + dir], g.V, ex.ctl, 13);
-    bq_push((unsigned)dir, !(o1 & bit), n1, w.qcap, w.Q[dir][par], &ex.ctl->lc[nxt][C_FQ + dir], g.V, ex.ctl, 13);
+    const bool c0 = !(o0 & bit), c1 = !(o1 & bit);
+    // edges the claimed vertices will expand next (direction-switch rule)
+    const uint32_t *Rn = dir ? g.Br : g.Fr;
+    unsigned e = 0;
+    if (c0) e += __ldg(&Rn[n0 + 1]) - __ldg(&Rn[n0]);
+    if (c1) e += __ldg(&Rn[n1 + 1]) - __ldg(&Rn[n1]);
+    bq_add_edges((unsigned)dir, e);
+    bq_push((unsigned)dir, c0, n0, w.qcap, w.Q[dir][par], &ex.ctl->lc[nxt][C_FQ + dir], g.V, ex.ctl, 13);
+    bq_push((unsigned)dir, c1, n1, w.qcap, w.Q[dir][par], &ex.ctl->lc[nxt][C_FQ + dir], g.V, ex.ctl, 13);
 }
 
 template <class Ex>
@@ -404,6 +470,10 @@ __device__ __forceinline__ void bfs_pull_group(Ex &ex, const Graph &g, const Wor
         }
     }
     if (found) atomicOr(&w.st[v], bit);
+    {
+        const uint32_t *Rn = dir ? g.Br : g.Fr;
+        bq_add_edges((unsigned)dir, found ? __ldg(&Rn[v + 1]) - __ldg(&Rn[v]) : 0u);
+    }
     count_verts(ex, valid);
     if constexpr (Ex::instr) {
         unsigned t = __reduce_add_sync(FULL, scanned);
@@ -432,7 +502,7 @@ struct SeedRoot {     // colouring roots (selectPivotColoring, scc_kernels.cu:56
 // the seed predicate, flags seeds and expands them.  Each later pass picks,
 // per direction, top-down (expand the frontier queue and the heavy chunks)
 // or bottom-up over `scope` (the vertices the search can reach) when the
-// frontier holds more than scope.n / bu_den vertices.  lw < 0 selects the
+// frontier's vertices have more than bu_k * scope.n edges to expand.  lw < 0 selects the
 // load-balanced warp schedule for top-down steps, lw >= 0 the virtual-warp
 // schedule with W = 1 << lw.
 template <class Ex, class Seed>
@@ -480,7 +550,8 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
             bfs_expand_lanes(ex, g, w, 0, v, act, r, lw, par, nxt);
             if (bw) bfs_expand_lanes(ex, g, w, 1, v, act, r, lw, par, nxt);
         }
-        bq_flush(2, w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_FQ], w.Q[1][par], &ex.ctl->lc[nxt][C_BQ], g.V, ex.ctl);
+        bq_flush(2, w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_FQ], w.Q[1][par], &ex.ctl->lc[nxt][C_BQ], g.V, ex.ctl,
+                 &ex.ctl->lc[nxt][C_FE], &ex.ctl->lc[nxt][C_BE]);
     });
     if (!ok) return false;
     const uint32_t nsg = (scope.n + 31u) / 32u;
@@ -489,8 +560,11 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
         const uint32_t nhf = last_count(ex, C_FH), nhb = last_count(ex, C_BH);
         if (nf + nb + nhf + nhb == 0u) return true;
         if (lev > g.V + 2u) { if (ex.leader()) set_error(ex.ctl, E_NOT_CONVERGED, 40); return false; }
-        const bool puf = w.bu_den && nf > scope.n / w.bu_den;
-        const bool pub = bw && w.bu_den && nb > scope.n / w.bu_den;
+        // Beamer's rule: bottom-up when the frontier has more edges to
+        // expand than the scope has vertices to test (times bu_k)
+        const uint32_t mf = last_count(ex, C_FE), mb = last_count(ex, C_BE);
+        const bool puf = w.bu_k && (unsigned long long)mf > (unsigned long long)scope.n * w.bu_k;
+        const bool pub = bw && w.bu_k && (unsigned long long)mb > (unsigned long long)scope.n * w.bu_k;
         ok = run_pass(ex, (puf || pub) ? PH_BFS_PULL : PH_BFS, [&](unsigned, unsigned nxt) {
             const unsigned par = ex.gl & 1u, cp = par ^ 1u;
             const uint32_t ngf = (nf + gsz - 1u) / gsz, ngb = (nb + gsz - 1u) / gsz;
@@ -525,7 +599,7 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
                 }
             }
             bq_flush(2, w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_FQ], w.Q[1][par], &ex.ctl->lc[nxt][C_BQ], g.V,
-                     ex.ctl);
+                     ex.ctl, &ex.ctl->lc[nxt][C_FE], &ex.ctl->lc[nxt][C_BE]);
         });
         if (!ok) return false;
     }
@@ -616,31 +690,33 @@ __device__ bool ph_hong_update(Ex &ex, const Graph &g, const Work &w, VList src,
                                bool single, bool fold)
 {
     return run_pass(ex, PH_HONG_UPDATE, [&](unsigned, unsigned nxt) {
-        for (uint32_t base = ex.wid() * 32u; base < src.n; base += ex.nwarps() * 32u) {
-            uint32_t i = base + lane_id();
-            bool valid = i < src.n, surv = false;
-            uint32_t v = valid ? src.at(i) : 0u, nr = 0u;
-            uint32_t p = 0u;
-            bool scc = false;
-            if (valid) {
-                uint32_t s = w.st[v];
-                if (s != DEAD) {
-                    p = key_vertex(w.pivkey[single ? 0u : (s & RMASK)]);
-                    if ((s & FVB) && (s & BVB)) {
-                        w.st[v] = DEAD;
-                        w.label[v] = p;
+        for (uint32_t base = ex.wid() * 128u; base < src.n; base += ex.nwarps() * 128u) {
+            uint32_t v[4], s[4];
+            bool ok[4];
+            load_list4(src, base + 4u * lane_id(), v, ok);
+#pragma unroll
+            for (int j = 0; j < 4; j++) s[j] = ok[j] ? w.st[v[j]] : DEAD;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                bool surv = false, scc = false;
+                uint32_t p = 0u, nr = 0u;
+                if (s[j] != DEAD) {
+                    p = key_vertex(w.pivkey[single ? 0u : (s[j] & RMASK)]);
+                    if ((s[j] & FVB) && (s[j] & BVB)) {
+                        w.st[v[j]] = DEAD;
+                        w.label[v[j]] = p;
                         scc = true;
                     } else {
-                        nr = split_name(g.V, p, s);
-                        w.st[v] = nr;
+                        nr = split_name(g.V, p, s[j]);
+                        w.st[v[j]] = nr;
                         surv = true;
                     }
                 }
+                smin_fold(scc, p, v[j], w.smin);
+                bq_push(0, surv, v[j], w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 15);
+                if (fold) range_max_atomic(surv, nr, surv ? pivot_key(g, v[j]) : 0ull, w.pivkey);
             }
-            count_verts(ex, valid);
-            smin_fold(scc, p, v, w.smin);
-            bq_push(0, surv, v, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 15);
-            if (fold) range_max_atomic(surv, nr, surv ? pivot_key(g, v) : 0ull, w.pivkey);
+            count_verts_n(ex, (unsigned)ok[0] + ok[1] + ok[2] + ok[3]);
         }
         bq_flush(1, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], nullptr, nullptr, g.V, ex.ctl);
     });
@@ -654,21 +730,23 @@ __device__ bool ph_slota_first_update(Ex &ex, const Graph &g, const Work &w, VLi
 {
     return run_pass(ex, PH_SLOTA_FIRST_UPDATE, [&](unsigned, unsigned nxt) {
         const uint32_t p = key_vertex(w.pivkey[0]);
-        for (uint32_t base = ex.wid() * 32u; base < src.n; base += ex.nwarps() * 32u) {
-            uint32_t i = base + lane_id();
-            bool valid = i < src.n, surv = false;
-            uint32_t v = valid ? src.at(i) : 0u;
-            bool scc = false;
-            if (valid) {
-                uint32_t s = w.st[v];
-                if (s != DEAD) {
-                    if ((s & FVB) && (s & BVB)) { w.st[v] = DEAD; w.label[v] = p; scc = true; }
-                    else { w.st[v] = v; surv = true; }
+        for (uint32_t base = ex.wid() * 128u; base < src.n; base += ex.nwarps() * 128u) {
+            uint32_t v[4], s[4];
+            bool ok[4];
+            load_list4(src, base + 4u * lane_id(), v, ok);
+#pragma unroll
+            for (int j = 0; j < 4; j++) s[j] = ok[j] ? w.st[v[j]] : DEAD;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                bool surv = false, scc = false;
+                if (s[j] != DEAD) {
+                    if ((s[j] & FVB) && (s[j] & BVB)) { w.st[v[j]] = DEAD; w.label[v[j]] = p; scc = true; }
+                    else { w.st[v[j]] = v[j]; surv = true; }
                 }
+                smin_fold(scc, p, v[j], w.smin);
+                bq_push(0, surv, v[j], w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 16);
             }
-            count_verts(ex, valid);
-            smin_fold(scc, p, v, w.smin);
-            bq_push(0, surv, v, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 16);
+            count_verts_n(ex, (unsigned)ok[0] + ok[1] + ok[2] + ok[3]);
         }
         bq_flush(1, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], nullptr, nullptr, g.V, ex.ctl);
     });
@@ -681,20 +759,24 @@ template <class Ex>
 __device__ bool ph_slota_peel_update(Ex &ex, const Graph &g, const Work &w, VList src, uint32_t *Lout)
 {
     return run_pass(ex, PH_SLOTA_PEEL_UPDATE, [&](unsigned, unsigned nxt) {
-        for (uint32_t base = ex.wid() * 32u; base < src.n; base += ex.nwarps() * 32u) {
-            uint32_t i = base + lane_id();
-            bool valid = i < src.n, surv = false;
-            uint32_t v = valid ? src.at(i) : 0u;
-            bool scc = false;
-            uint32_t c = 0u;
-            if (valid) {
-                uint32_t s = w.st[v];
-                if (s & FVB) { c = s & RMASK; w.st[v] = DEAD; w.label[v] = c; scc = true; }
-                else { w.st[v] = v; surv = true; }
+        for (uint32_t base = ex.wid() * 128u; base < src.n; base += ex.nwarps() * 128u) {
+            uint32_t v[4], s[4];
+            bool ok[4];
+            load_list4(src, base + 4u * lane_id(), v, ok);
+#pragma unroll
+            for (int j = 0; j < 4; j++) s[j] = ok[j] ? w.st[v[j]] : 0u;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                bool surv = false, scc = false;
+                uint32_t c = 0u;
+                if (ok[j]) {
+                    if (s[j] & FVB) { c = s[j] & RMASK; w.st[v[j]] = DEAD; w.label[v[j]] = c; scc = true; }
+                    else { w.st[v[j]] = v[j]; surv = true; }
+                }
+                smin_fold(scc, c, v[j], w.smin);
+                bq_push(0, surv, v[j], w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 17);
             }
-            count_verts(ex, valid);
-            smin_fold(scc, c, v, w.smin);
-            bq_push(0, surv, v, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 17);
+            count_verts_n(ex, (unsigned)ok[0] + ok[1] + ok[2] + ok[3]);
         }
         bq_flush(1, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], nullptr, nullptr, g.V, ex.ctl);
     });
@@ -707,13 +789,19 @@ template <class Ex>
 __device__ bool ph_compact_rename(Ex &ex, const Graph &g, const Work &w, VList src, uint32_t *Lout)
 {
     return run_pass(ex, PH_RENAME, [&](unsigned, unsigned nxt) {
-        for (uint32_t base = ex.wid() * 32u; base < src.n; base += ex.nwarps() * 32u) {
-            uint32_t i = base + lane_id();
-            bool valid = i < src.n, surv = false;
-            uint32_t v = valid ? src.at(i) : 0u;
-            if (valid && w.st[v] != DEAD) { w.st[v] = v; surv = true; }
-            count_verts(ex, valid);
-            bq_push(0, surv, v, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 18);
+        for (uint32_t base = ex.wid() * 128u; base < src.n; base += ex.nwarps() * 128u) {
+            uint32_t v[4], s[4];
+            bool ok[4];
+            load_list4(src, base + 4u * lane_id(), v, ok);
+#pragma unroll
+            for (int j = 0; j < 4; j++) s[j] = ok[j] ? w.st[v[j]] : DEAD;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const bool surv = s[j] != DEAD;
+                if (surv) w.st[v[j]] = v[j];
+                bq_push(0, surv, v[j], w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 18);
+            }
+            count_verts_n(ex, (unsigned)ok[0] + ok[1] + ok[2] + ok[3]);
         }
         bq_flush(1, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], nullptr, nullptr, g.V, ex.ctl);
     });
@@ -772,15 +860,26 @@ __device__ bool ph_first_pivot(Ex &ex, const Graph &g, const Work &w, uint32_t *
 {
     return run_pass(ex, PH_FIRST_PIVOT, [&](unsigned, unsigned nxt) {
         unsigned long long best = 0;
-        for (uint32_t base = ex.wid() * 32u; base < g.V; base += ex.nwarps() * 32u) {
-            const uint32_t v = base + lane_id() + 1u;
-            const bool live = v <= g.V && w.st[v] != DEAD;
-            if (live) {
-                unsigned long long k = pivot_key(g, v);
-                best = k > best ? k : best;
+        for (uint32_t base = ex.wid() * 128u; base <= g.V; base += ex.nwarps() * 128u) {
+            const uint32_t i0 = base + 4u * lane_id();
+            uint32_t st4[4] = {DEAD, DEAD, DEAD, DEAD};
+            if (i0 + 3u <= g.V) {
+                const uint4 x = *reinterpret_cast<const uint4 *>(w.st + i0);
+                st4[0] = x.x; st4[1] = x.y; st4[2] = x.z; st4[3] = x.w;
+            } else {
+                for (uint32_t j = 0; j < 4u && i0 + j <= g.V; j++) st4[j] = w.st[i0 + j];
             }
-            count_verts(ex, v <= g.V);
-            bq_push(0, live, v, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 20);
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const uint32_t v = i0 + (uint32_t)j;
+                const bool live = v >= 1u && v <= g.V && st4[j] != DEAD;
+                if (live) {
+                    unsigned long long k = pivot_key(g, v);
+                    best = k > best ? k : best;
+                }
+                bq_push(0, live, v, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 20);
+            }
+            count_verts_n(ex, i0 <= g.V ? min(4u, g.V + 1u - i0) : 0u);
         }
         block_max_atomic(best, &w.pivkey[0]);
         bq_flush(1, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], nullptr, nullptr, g.V, ex.ctl);

@@ -115,8 +115,9 @@ int scc_run(scc_context *ctx, const scc_csr_view *g, int algo, uint32_t flags, i
  *   "timeout_ms"          bound on any grid-barrier wait (default 4000)
  *   "max_blocks_per_sm"   cap on CTAs per SM of the persistent launch
  *   "trace"               record a per-pass trace of up to `value` passes
- *   "bu_den"              bottom-up BFS step when the frontier exceeds
- *                         scope / bu_den vertices (default 16, 0 = never)
+ *   "bu_k"                bottom-up BFS step when the frontier's edges exceed
+ *                         bu_k * (vertices the search can reach) (default 1,
+ *                         0 = never)
  *   "qcap"                entries of each per-CTA shared-memory staging queue */
 int scc_set_tuning(scc_context *ctx, const char *key, long long value);
 
