@@ -103,10 +103,13 @@ struct Work {
     uint32_t bu_k;              // bottom-up BFS step when frontier edges > bu_k * scope vertices (0 = never)
 };
 
-// Dynamic shared memory of the SCC kernels: 16 control words, then NBQ
-// staging queues of qcap entries each.
+// Dynamic shared memory of the SCC kernels: BQ_HDR control words, then NBQ
+// staging queues, each split into one slice of qcap entries per warp.
 constexpr unsigned NBQ = 2;
-constexpr unsigned BQ_WORDS = 16;
+constexpr unsigned BQ_WARPS = 32;                       // at most 1024 threads per CTA
+constexpr unsigned BQ_CNT = 16;                         // per-warp fill counts [NBQ][BQ_WARPS]
+constexpr unsigned BQ_PRE = BQ_CNT + NBQ * BQ_WARPS;    // per-warp flush offsets [NBQ][BQ_WARPS]
+constexpr unsigned BQ_HDR = BQ_PRE + NBQ * BQ_WARPS;
 extern __shared__ uint32_t sccb_dsmem[];
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
@@ -264,31 +267,42 @@ __device__ __forceinline__ void warp_push(bool pred, uint32_t val, uint32_t *q, 
     }
 }
 
-// CTA-level staging of queue appends: lanes append into a shared-memory
-// buffer (one shared atomic per warp); bq_flush copies the buffer to the
-// global queue with one global atomicAdd per CTA and pass.  Appends beyond
-// the buffer go straight to the global queue.  This keeps the global queue
-// tail from becoming a same-address atomic hot spot (one per warp step).
+// Staging of queue appends in shared memory: every warp appends into its
+// own slice (warp ballot, no atomics); a full slice is written out by its
+// warp with one global atomicAdd per qcap entries, and bq_flush writes the
+// rest of all slices with one global atomicAdd per CTA and pass.  This keeps
+// the global queue tail from becoming a same-address atomic hot spot.
 __device__ __forceinline__ void bq_init()
 {
-    if (threadIdx.x < BQ_WORDS) sccb_dsmem[threadIdx.x] = 0u;
+    for (unsigned i = threadIdx.x; i < BQ_HDR; i += blockDim.x) sccb_dsmem[i] = 0u;
     __syncthreads();
 }
 
 __device__ __forceinline__ void bq_push(unsigned qi, bool pred, uint32_t val, uint32_t qcap, uint32_t *gq,
                                         unsigned *gcnt, uint32_t gcap, Ctl *ctl, int where)
 {
-    unsigned m = __ballot_sync(FULL, pred);
+    const unsigned m = __ballot_sync(FULL, pred);
     if (m == 0u) return;
-    unsigned lane = lane_id();
-    unsigned ld = __ffs(m) - 1u;
-    unsigned base = 0;
-    if (lane == ld) base = atomicAdd(&sccb_dsmem[qi], (unsigned)__popc(m));
-    base = __shfl_sync(FULL, base, ld);
-    unsigned pos = base + __popc(m & ((1u << lane) - 1u));
-    bool spill = pred && pos >= qcap;
-    if (pred && !spill) sccb_dsmem[BQ_WORDS + qi * qcap + pos] = val;
-    warp_push(spill, val, gq, gcnt, gcap, ctl, where);
+    const unsigned lane = lane_id(), wi = threadIdx.x >> 5;
+    uint32_t *slice = &sccb_dsmem[BQ_HDR + (qi * BQ_WARPS + wi) * qcap];
+    unsigned *wc = &sccb_dsmem[BQ_CNT + qi * BQ_WARPS + wi];
+    unsigned cnt = *wc;
+    const unsigned n = __popc(m);
+    if (cnt + n > qcap) {
+        unsigned base = 0;
+        if (lane == 0) base = atomicAdd(gcnt, cnt);
+        base = __shfl_sync(FULL, base, 0);
+        for (unsigned i = lane; i < cnt; i += 32u) {
+            if (base + i < gcap) gq[base + i] = slice[i];
+            else set_error(ctl, E_OVERFLOW, where);
+        }
+        __syncwarp();
+        cnt = 0;
+    }
+    if (pred) slice[cnt + __popc(m & ((1u << lane) - 1u))] = val;
+    __syncwarp();
+    if (lane == 0) *wc = cnt + n;
+    __syncwarp();
 }
 
 // Adds x to the CTA's frontier-edge tally of queue qi (words 12, 13).
@@ -305,26 +319,33 @@ __device__ __forceinline__ void bq_flush(unsigned nq, uint32_t qcap, uint32_t *g
                                          unsigned *ecnt1 = nullptr)
 {
     __syncthreads();
+    const unsigned nw = blockDim.x >> 5;
     if (threadIdx.x == 0) {
         for (unsigned qi = 0; qi < nq; qi++) {
-            unsigned n = min(sccb_dsmem[qi], qcap);
-            sccb_dsmem[4 + qi] = n;
-            sccb_dsmem[8 + qi] = n ? atomicAdd(qi ? gcnt1 : gcnt0, n) : 0u;
-            sccb_dsmem[qi] = 0u;
+            unsigned total = 0;
+            for (unsigned wi = 0; wi < nw; wi++) {
+                sccb_dsmem[BQ_PRE + qi * BQ_WARPS + wi] = total;
+                total += sccb_dsmem[BQ_CNT + qi * BQ_WARPS + wi];
+            }
+            sccb_dsmem[8 + qi] = total ? atomicAdd(qi ? gcnt1 : gcnt0, total) : 0u;
             unsigned *ec = qi ? ecnt1 : ecnt0;
             if (ec && sccb_dsmem[12 + qi]) atomicAdd(ec, sccb_dsmem[12 + qi]);
             sccb_dsmem[12 + qi] = 0u;
         }
     }
     __syncthreads();
+    const unsigned wi = threadIdx.x >> 5;
     for (unsigned qi = 0; qi < nq; qi++) {
-        const unsigned n = sccb_dsmem[4 + qi], base = sccb_dsmem[8 + qi];
         uint32_t *gq = qi ? gq1 : gq0;
-        const uint32_t *buf = &sccb_dsmem[BQ_WORDS + qi * qcap];
-        for (unsigned i = threadIdx.x; i < n; i += blockDim.x) {
-            if (base + i < gcap) gq[base + i] = buf[i];
+        const unsigned cnt = sccb_dsmem[BQ_CNT + qi * BQ_WARPS + wi];
+        const unsigned base = sccb_dsmem[8 + qi] + sccb_dsmem[BQ_PRE + qi * BQ_WARPS + wi];
+        const uint32_t *slice = &sccb_dsmem[BQ_HDR + (qi * BQ_WARPS + wi) * qcap];
+        for (unsigned i = lane_id(); i < cnt; i += 32u) {
+            if (base + i < gcap) gq[base + i] = slice[i];
             else set_error(ctl, E_OVERFLOW, 3);
         }
+        __syncwarp();
+        if (lane_id() == 0) sccb_dsmem[BQ_CNT + qi * BQ_WARPS + wi] = 0u;
     }
 }
 
@@ -430,7 +451,14 @@ __device__ __forceinline__ unsigned lbs_expand2(uint32_t beg, uint32_t deg, uint
 // stored value is already smaller.  All 32 lanes call.
 __device__ __forceinline__ void smin_fold(bool valid, uint32_t rep, uint32_t v, uint32_t *smin)
 {
-    if (__ballot_sync(FULL, valid) == 0u) return;
+    const unsigned vm = __ballot_sync(FULL, valid);
+    if (vm == 0u) return;
+    const uint32_t rep0 = __shfl_sync(FULL, rep, __ffs(vm) - 1);
+    if (__all_sync(FULL, !valid || rep == rep0)) {   // one SCC for the whole warp (the common case)
+        const uint32_t mn = __reduce_min_sync(FULL, valid ? v : 0xFFFFFFFFu);
+        if (lane_id() == 0 && mn < vld(&smin[rep0])) atomicMin(&smin[rep0], mn);
+        return;
+    }
     unsigned grp = __match_any_sync(FULL, valid ? rep : 0xFFFFFFFFu);
     uint32_t mn = __reduce_min_sync(grp, valid ? v : 0xFFFFFFFFu);
     if (valid && lane_id() == (unsigned)(__ffs(grp) - 1) && mn < vld(&smin[rep])) atomicMin(&smin[rep], mn);

@@ -36,7 +36,7 @@ struct Params {
 constexpr int GRID_THREADS = 1024;
 constexpr int BLOCK_THREADS = 1024;
 
-static size_t dyn_smem_bytes(uint32_t qcap) { return (BQ_WORDS + NBQ * (size_t)qcap) * sizeof(uint32_t); }
+static size_t dyn_smem_bytes(uint32_t qcap) { return (BQ_HDR + NBQ * BQ_WARPS * (size_t)qcap) * sizeof(uint32_t); }
 
 template <bool INSTR, bool HONG>
 __global__ void __launch_bounds__(GRID_THREADS, 1) k_scc_grid(Params p)
@@ -404,7 +404,7 @@ extern "C" int scc_set_tuning(scc_context *ctx, const char *key, long long value
     else if (!strcmp(key, "max_blocks_per_sm")) ctx->max_blocks_per_sm = (int)value;
     else if (!strcmp(key, "bu_k")) ctx->bu_k = (uint32_t)value;
     else if (!strcmp(key, "qcap")) {
-        if (value < 256 || value > 24576) return SCC_ERR_INVALID_ARG;
+        if (value < 32 || value > 768) return SCC_ERR_INVALID_ARG;
         ctx->qcap = (uint32_t)value;
     } else if (!strcmp(key, "trace")) {
         // per-pass trace of the next runs: `value` passes (0 switches it off)

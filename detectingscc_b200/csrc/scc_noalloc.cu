@@ -38,7 +38,7 @@ int sccb_launch_block_path(const Graph &g, const Work &w, int t1, int t2, int lw
 
 namespace {
 
-constexpr uint32_t NOALLOC_QCAP = 8192;
+constexpr uint32_t NOALLOC_QCAP = 512;
 
 constexpr size_t al256(size_t x) { return (x + 255) / 256 * 256; }
 

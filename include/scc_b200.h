@@ -118,7 +118,8 @@ int scc_run(scc_context *ctx, const scc_csr_view *g, int algo, uint32_t flags, i
  *   "bu_k"                bottom-up BFS step when the frontier's edges exceed
  *                         bu_k * (vertices the search can reach) (default 1,
  *                         0 = never)
- *   "qcap"                entries of each per-CTA shared-memory staging queue */
+ *   "qcap"                entries of each warp's shared-memory staging slice
+ *                         (32..768; 2 queues x 32 warps x qcap x 4 bytes) */
 int scc_set_tuning(scc_context *ctx, const char *key, long long value);
 
 /* Per-pass trace of the last run (enable with scc_set_tuning(ctx, "trace",
