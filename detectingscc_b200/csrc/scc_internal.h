@@ -32,7 +32,7 @@ struct scc_context {
     uint32_t timeout_ms = 4000;          // bound on any single grid-barrier wait
     int max_blocks_per_sm = 0;           // 0 = occupancy limit
     uint32_t qcap = 512;                 // per-warp staging slice entries (2 queues x 32 warps in shared memory)
-    uint32_t bu_k = 1;                   // bottom-up BFS step when frontier edges > bu_k * scope (0 = off)
+    uint32_t bu_k = 2;                   // bottom-up BFS step when frontier edges > bu_k * scope (0 = off)
 
     // optional per-pass trace
     unsigned long long *dtrace = nullptr, *htrace = nullptr;

@@ -147,7 +147,7 @@ extern "C" int scc_run_noalloc(const scc_csr_view *gv, int algo, uint32_t flags,
     w.pivkey = (unsigned long long *)take((4 * n1 + 8) * 8);
     w.ctl = (Ctl *)take(sizeof(Ctl));
     w.qcap = NOALLOC_QCAP;
-    w.bu_k = 1;
+    w.bu_k = 2;
     if (off > NOALLOC_BYTES) return SCC_ERR_TOO_LARGE;
 
     cudaStream_t st = (cudaStream_t)stream;

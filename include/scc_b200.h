@@ -116,7 +116,7 @@ int scc_run(scc_context *ctx, const scc_csr_view *g, int algo, uint32_t flags, i
  *   "max_blocks_per_sm"   cap on CTAs per SM of the persistent launch
  *   "trace"               record a per-pass trace of up to `value` passes
  *   "bu_k"                bottom-up BFS step when the frontier's edges exceed
- *                         bu_k * (vertices the search can reach) (default 1,
+ *                         bu_k * (vertices the search can reach) (default 2,
  *                         0 = never)
  *   "qcap"                entries of each warp's shared-memory staging slice
  *                         (32..768; 2 queues x 32 warps x qcap x 4 bytes) */
