@@ -62,13 +62,15 @@ FLAG_DEVICE = 0x4
 FLAG_INSTRUMENT = 0x8
 FLAG_FORCE_GRID = 0x10
 FLAG_FORCE_BLOCK = 0x20
+FLAG_BATCH_SEQUENTIAL = 0x40
 MAX_VERTICES = 268435454
 
 # every symbol include/scc_b200.h and include/scc_compat.h declare
 C_SYMBOLS = ["scc_create", "scc_destroy", "scc_run", "scc_set_tuning", "scc_status_string",
              "scc_version", "scc_get_trace", "scc_load_graph", "scc_save_binary", "scc_graph_from_arcs",
              "scc_free_host_graph", "scc_reference_call", "scc_batch_create", "scc_batch_run",
-             "scc_batch_destroy", "scc_run_noalloc"]
+             "scc_batch_destroy", "scc_run_noalloc", "scc_batch_set_schedule", "scc_batch_get_schedule",
+             "scc_batch_autotune", "scc_batch_info"]
 CXX_SYMBOLS = ["_Z5vHongjjPjS_S_S_bb", "_Z6vSlotajjPjS_S_S_bb", "_Z5wHongjjPjS_S_S_bbi",
                "_Z6wSlotajjPjS_S_S_bbi", "_Z13loadFullGraphPKcPjS1_PS1_S2_S2_S2_S2_"]
 
@@ -115,6 +117,11 @@ def lib():
     L.scc_batch_run.argtypes = [vp, ctypes.c_int, u32, ctypes.c_int, vp, ctypes.POINTER(BatchResult),
                                 ctypes.POINTER(Stats)]
     L.scc_batch_destroy.argtypes = [vp]
+    L.scc_batch_set_schedule.argtypes = [vp, ctypes.c_int, u32]
+    L.scc_batch_get_schedule.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(u32)]
+    L.scc_batch_autotune.argtypes = [vp, ctypes.c_int, u32, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                     ctypes.POINTER(u32), ctypes.POINTER(ctypes.c_float)]
+    L.scc_batch_info.argtypes = [vp, ctypes.POINTER(u64), ctypes.POINTER(u64), ctypes.POINTER(u32)]
     L.scc_run_noalloc.argtypes = [ctypes.POINTER(CsrView), ctypes.c_int, u32, ctypes.c_int, vp,
                                   ctypes.POINTER(Stats), vp]
     L.scc_get_trace.argtypes = [vp, ctypes.POINTER(u64), u32, ctypes.POINTER(u32), ctypes.POINTER(u64)]

@@ -170,6 +170,69 @@ class Engine:
         return Result(None, st.num_sccs, st.num_trim1, st.num_trim2, st.num_pivot, st.as_dict())
 
 
+class Batch:
+    """Many independent graphs resident on one device, run in one launch."""
+
+    def __init__(self, engine: "Engine", graphs):
+        self._lib = engine._lib
+        self.engine = engine
+        self.graphs = list(graphs)
+        self._keep = self.graphs  # host arrays must outlive the upload only; kept for offsets
+        views = (N.CsrView * max(len(self.graphs), 1))()
+        for i, g in enumerate(self.graphs):
+            views[i] = N.CsrView(g.V, g.E, _ptr(g.Fr), _ptr(g.Fc), _ptr(g.Br), _ptr(g.Bc))
+        h = ctypes.c_void_p()
+        N.check(self._lib.scc_batch_create(engine._h, views, len(self.graphs), ctypes.byref(h)), "scc_batch_create")
+        self._h = h
+        self.offsets = np.concatenate([[0], np.cumsum([g.V for g in self.graphs])]).astype(np.int64)
+        self.total_vertices = int(self.offsets[-1])
+        self.total_edges = int(sum(g.E for g in self.graphs))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.scc_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_schedule(self, threads: int, qcap: int) -> None:
+        N.check(self._lib.scc_batch_set_schedule(self._h, int(threads), int(qcap)), "scc_batch_set_schedule")
+
+    def schedule(self):
+        t, q = ctypes.c_int(0), ctypes.c_uint32(0)
+        N.check(self._lib.scc_batch_get_schedule(self._h, ctypes.byref(t), ctypes.byref(q)))
+        return t.value, q.value
+
+    def autotune(self, algo="h", t1=True, t2=True, warp=1):
+        t, q, ms = ctypes.c_int(0), ctypes.c_uint32(0), ctypes.c_float(0)
+        flags = (N.FLAG_TRIM1 if t1 else 0) | (N.FLAG_TRIM2 if t2 else 0)
+        N.check(self._lib.scc_batch_autotune(self._h, _algo_code(algo), flags, int(warp), ctypes.byref(t),
+                                             ctypes.byref(q), ctypes.byref(ms)), "scc_batch_autotune")
+        return t.value, q.value, ms.value
+
+    def run(self, algo="h", t1=True, t2=True, warp=1, labels=True, sequential=False, out=None, check=True):
+        """Returns (labels concatenated in batch order or None, per-graph results, stats)."""
+        flags = (N.FLAG_TRIM1 if t1 else 0) | (N.FLAG_TRIM2 if t2 else 0)
+        flags |= N.FLAG_BATCH_SEQUENTIAL if sequential else 0
+        if labels and out is None:
+            out = np.zeros(max(self.total_vertices, 1), dtype=np.uint32)
+        res = (N.BatchResult * max(len(self.graphs), 1))()
+        st = N.Stats()
+        rc = self._lib.scc_batch_run(self._h, _algo_code(algo), flags, int(warp), _ptr(out) if labels else None,
+                                     res, ctypes.byref(st))
+        if check:
+            N.check(rc, "scc_batch_run")
+        results = [(int(r.num_sccs), int(r.num_trim1), int(r.status)) for r in res[:len(self.graphs)]]
+        return (out[:self.total_vertices] if labels else None), results, st.as_dict()
+
+    def labels_of(self, labels, i):
+        return labels[self.offsets[i]:self.offsets[i + 1]]
+
+
 # ----------------------------------------------------------------------
 # graph files
 # ----------------------------------------------------------------------

@@ -1,13 +1,449 @@
-// Batched form (placeholder until the batch kernel lands).
-#include "../../include/scc_b200.h"
+// Batched form: thousands of independent graphs in one persistent launch.
+//
+// The graphs are uploaded once into one arena (packed CSR arrays).  One
+// launch of k_scc_batch runs them all: every CTA takes the next graph from
+// a work counter (graphs ordered largest first, so the long ones start
+// early), re-carves its private scratch for that graph and runs the same
+// driver code as the plain path with the single-CTA execution policy
+// (BlockExec), then writes the graph's canonical labels and counters.  SCCs
+// never cross graphs, so graphs need no coordination.  The launch (counter
+// reset + kernel) is captured once into a CUDA graph and replayed.
+//
+// SCC_FLAG_BATCH_SEQUENTIAL runs the same graphs as per-graph plain calls
+// (scc_run on device pointers into the arena, one after the other on one
+// stream): the baseline the batched launch is measured against.
+//
+// Schedules (CTA size 128 / 256 / 512 / 1024 threads, staging slice size)
+// are picked by scc_batch_autotune, which times candidates on the batch.
+#include <cuda_runtime.h>
 
-extern "C" int scc_batch_create(scc_context *, const scc_csr_view *, uint32_t, scc_batch **out)
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <numeric>
+#include <vector>
+
+#include "../../include/scc_b200.h"
+#include "scc_internal.h"
+#include "scc_phases.cuh"
+
+using namespace sccb;
+
+namespace {
+
+struct BatchGraph {
+    uint32_t V, E;
+    unsigned long long off_r;   // into the packed Fr / Br arrays (V+2 entries per graph)
+    unsigned long long off_c;   // into the packed Fc / Bc arrays
+    unsigned long long off_out; // into the packed label output (V entries per graph)
+};
+
+struct BatchRes {
+    unsigned long long trim1, trim2, pivot;
+    int status, where;
+};
+
+struct BatchParams {
+    const BatchGraph *graphs;
+    const uint32_t *order;
+    uint32_t n;
+    const uint32_t *Fr, *Fc, *Br, *Bc;
+    uint32_t vec;
+    uint32_t *out;
+    BatchRes *res;
+    char *scratch;
+    unsigned long long scratch_per_cta;
+    unsigned *next;
+    uint32_t qcap, bu_k;
+    int t1, t2, lw;
+    unsigned long long timeout_ns;
+};
+
+template <int THREADS, bool HONG>
+__global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_scc_batch(BatchParams p)
 {
-    if (out) *out = nullptr;
-    return SCC_ERR_INVALID_ARG;
+    __shared__ uint32_t s_k;
+    __shared__ Work s_w;   // per-graph carving, kept in shared memory rather than local memory
+    bq_init();
+    char *mine = p.scratch + (size_t)blockIdx.x * p.scratch_per_cta;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_k = atomicAdd(p.next, 1u);
+        __syncthreads();
+        const uint32_t k = s_k;
+        if (k >= p.n) return;
+        const uint32_t gi = p.order[k];
+        const BatchGraph bg = p.graphs[gi];
+        if (bg.V == 0u) {
+            if (threadIdx.x == 0) p.res[gi] = BatchRes{0ull, 0ull, 0ull, 0, 0};
+            continue;
+        }
+        Graph g{bg.V, bg.E, p.Fr + bg.off_r, p.Fc + bg.off_c, p.Br + bg.off_r, p.Bc + bg.off_c, p.vec};
+        if (threadIdx.x == 0) {
+            carve_work(mine, bg.V, bg.E, HONG, &s_w);
+            s_w.qcap = p.qcap;
+            s_w.bu_k = p.bu_k;
+        }
+        __syncthreads();
+        const Work &w = s_w;
+        // fresh control block and pivot table for this graph
+        {
+            uint32_t *c = reinterpret_cast<uint32_t *>(w.ctl);
+            for (unsigned i = threadIdx.x; i < sizeof(Ctl) / 4; i += blockDim.x) c[i] = 0u;
+            const uint32_t npk = HONG ? 4u * (bg.V + 1u) + 8u : 1u;
+            for (uint32_t i = threadIdx.x; i < npk; i += blockDim.x) w.pivkey[i] = 0ull;
+            __syncthreads();
+            if (threadIdx.x == 0) w.ctl->timeout_ns = p.timeout_ns;
+            __syncthreads();
+        }
+        BlockExec<false> ex{w.ctl, 0u};
+        Carry cy{0u, 0u, 0u};
+        int rc = HONG ? hong_front(ex, g, w, p.t1, p.t2, p.lw, cy) : slota_front(ex, g, w, p.t1, p.lw, cy);
+        if (rc == RUN_DONE) rc = HONG ? hong_loop(ex, g, w, cy, 0u) : slota_peels(ex, g, w, cy, 0u);
+        __syncthreads();
+        const int err = *(volatile int *)&w.ctl->error;
+        if (!err) {
+            uint32_t *o = p.out + bg.off_out;
+            for (uint32_t v = threadIdx.x + 1u; v <= bg.V; v += blockDim.x) {
+                const uint32_t l = w.label[v];
+                o[v - 1u] = l <= bg.V ? w.smin[l] : 0u;
+            }
+        }
+        if (threadIdx.x == 0)
+            p.res[gi] = BatchRes{w.ctl->n_trim1, w.ctl->n_trim2, w.ctl->n_pivot, err, w.ctl->where};
+    }
 }
-extern "C" int scc_batch_run(scc_batch *, int, uint32_t, int, uint32_t *, scc_batch_result *, scc_stats *)
+
+template <int THREADS>
+void *batch_kernel(bool hong)
 {
-    return SCC_ERR_INVALID_ARG;
+    return hong ? (void *)k_scc_batch<THREADS, true> : (void *)k_scc_batch<THREADS, false>;
 }
-extern "C" int scc_batch_destroy(scc_batch *) { return SCC_OK; }
+
+void *pick_batch_kernel(int threads, bool hong)
+{
+    switch (threads) {
+    case 128: return batch_kernel<128>(hong);
+    case 256: return batch_kernel<256>(hong);
+    case 512: return batch_kernel<512>(hong);
+    default: return batch_kernel<1024>(hong);
+    }
+}
+
+size_t batch_smem(int threads, uint32_t qcap) { return (BQ_HDR + NBQ * (size_t)(threads / 32) * qcap) * 4; }
+
+}  // namespace
+
+struct scc_batch {
+    scc_context *ctx = nullptr;
+    uint32_t n = 0;
+    unsigned long long sumV = 0, sumE = 0, sumR = 0;
+    uint32_t maxV = 0, maxE = 0;
+    uint32_t *dFr = nullptr, *dFc = nullptr, *dBr = nullptr, *dBc = nullptr, *dout = nullptr, *dorder = nullptr;
+    BatchGraph *dgraphs = nullptr;
+    std::vector<BatchGraph> hgraphs;
+    BatchRes *dres = nullptr, *hres = nullptr;
+    unsigned *dnext = nullptr;
+    char *scratch = nullptr;
+    size_t scratch_bytes = 0, scratch_per_cta = 0;
+    uint32_t ncta = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    int threads = 256;
+    uint32_t qcap = 256;
+    // captured launch
+    cudaGraphExec_t gexec = nullptr;
+    int g_algo = 0, g_w = 0, g_threads = 0;
+    uint32_t g_flags = 0, g_qcap = 0;
+};
+
+static void batch_free(scc_batch *b)
+{
+    if (!b) return;
+    if (b->gexec) cudaGraphExecDestroy(b->gexec);
+    cudaFree(b->dFr); cudaFree(b->dFc); cudaFree(b->dBr); cudaFree(b->dBc); cudaFree(b->dout);
+    cudaFree(b->dorder); cudaFree(b->dgraphs); cudaFree(b->dres); cudaFree(b->dnext); cudaFree(b->scratch);
+    if (b->hres) cudaFreeHost(b->hres);
+    for (auto &e : b->ev) if (e) cudaEventDestroy(e);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+// Scratch for the resident CTAs of the current schedule (grown on demand).
+static int batch_reserve_scratch(scc_batch *b, int threads, uint32_t qcap)
+{
+    void *fn = pick_batch_kernel(threads, true);
+    const size_t smem = batch_smem(threads, qcap);
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+        cudaFuncSetAttribute(pick_batch_kernel(threads, false), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess) {
+        cudaGetLastError();
+        return SCC_ERR_CUDA;
+    }
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, threads, smem) != cudaSuccess || occ <= 0) {
+        cudaGetLastError();
+        return SCC_ERR_CUDA;
+    }
+    const uint32_t ncta = (uint32_t)std::min<unsigned long long>((unsigned long long)occ * b->ctx->nsm, b->n ? b->n : 1);
+    const size_t need = (size_t)ncta * b->scratch_per_cta;
+    if (need > b->scratch_bytes) {
+        cudaFree(b->scratch);
+        b->scratch = nullptr;
+        b->scratch_bytes = 0;
+        if (cudaMalloc((void **)&b->scratch, need) != cudaSuccess) {
+            cudaGetLastError();
+            return SCC_ERR_OOM;
+        }
+        b->scratch_bytes = need;
+    }
+    b->ncta = ncta;
+    return SCC_OK;
+}
+
+extern "C" int scc_batch_create(scc_context *ctx, const scc_csr_view *graphs, uint32_t n, scc_batch **out)
+{
+    if (!ctx || !out || (n && !graphs)) return SCC_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return SCC_ERR_NO_DEVICE;
+    scc_batch *b = new (std::nothrow) scc_batch();
+    if (!b) return SCC_ERR_OOM;
+    b->ctx = ctx;
+    b->n = n;
+    b->hgraphs.resize(n);
+    for (uint32_t i = 0; i < n; i++) {
+        const scc_csr_view &g = graphs[i];
+        if (g.num_vertices > SCC_MAX_VERTICES || g.num_edges > SCC_MAX_EDGES) { batch_free(b); return SCC_ERR_TOO_LARGE; }
+        if (!g.Fr || !g.Br || (g.num_edges && (!g.Fc || !g.Bc))) { batch_free(b); return SCC_ERR_INVALID_ARG; }
+        b->hgraphs[i] = BatchGraph{g.num_vertices, g.num_edges, b->sumR, b->sumE, b->sumV};
+        b->sumR += (unsigned long long)g.num_vertices + 2;
+        b->sumE += g.num_edges;
+        b->sumV += g.num_vertices;
+        b->maxV = std::max(b->maxV, g.num_vertices);
+        b->maxE = std::max(b->maxE, g.num_edges);
+    }
+    // pad each packed array so every graph's offsets stay 16-byte aligned is not
+    // required: 128-bit offset loads are only used when the batch is aligned
+    int rc = SCC_OK;
+    auto alloc = [&](void **p, size_t bytes) {
+        if (rc != SCC_OK) return;
+        if (cudaMalloc(p, std::max<size_t>(bytes, 16)) != cudaSuccess) { cudaGetLastError(); rc = SCC_ERR_OOM; }
+    };
+    alloc((void **)&b->dFr, b->sumR * 4);
+    alloc((void **)&b->dBr, b->sumR * 4);
+    alloc((void **)&b->dFc, b->sumE * 4);
+    alloc((void **)&b->dBc, b->sumE * 4);
+    alloc((void **)&b->dout, b->sumV * 4);
+    alloc((void **)&b->dorder, (size_t)n * 4);
+    alloc((void **)&b->dgraphs, (size_t)n * sizeof(BatchGraph));
+    alloc((void **)&b->dres, (size_t)n * sizeof(BatchRes));
+    alloc((void **)&b->dnext, 4);
+    if (rc == SCC_OK && cudaMallocHost((void **)&b->hres, std::max<size_t>((size_t)n * sizeof(BatchRes), 16)) != cudaSuccess)
+        rc = SCC_ERR_OOM;
+    if (rc == SCC_OK && (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+                         cudaEventCreate(&b->ev[0]) != cudaSuccess || cudaEventCreate(&b->ev[1]) != cudaSuccess))
+        rc = SCC_ERR_CUDA;
+    if (rc != SCC_OK) { cudaGetLastError(); batch_free(b); return rc; }
+    for (uint32_t i = 0; i < n && rc == SCC_OK; i++) {
+        const scc_csr_view &g = graphs[i];
+        const BatchGraph &bg = b->hgraphs[i];
+        if (cudaMemcpyAsync(b->dFr + bg.off_r, g.Fr, ((size_t)g.num_vertices + 2) * 4, cudaMemcpyHostToDevice, b->stream) != cudaSuccess ||
+            cudaMemcpyAsync(b->dBr + bg.off_r, g.Br, ((size_t)g.num_vertices + 2) * 4, cudaMemcpyHostToDevice, b->stream) != cudaSuccess)
+            rc = SCC_ERR_CUDA;
+        if (g.num_edges && rc == SCC_OK &&
+            (cudaMemcpyAsync(b->dFc + bg.off_c, g.Fc, (size_t)g.num_edges * 4, cudaMemcpyHostToDevice, b->stream) != cudaSuccess ||
+             cudaMemcpyAsync(b->dBc + bg.off_c, g.Bc, (size_t)g.num_edges * 4, cudaMemcpyHostToDevice, b->stream) != cudaSuccess))
+            rc = SCC_ERR_CUDA;
+    }
+    // largest graphs first (longest-processing-time order)
+    std::vector<uint32_t> order(n);
+    std::iota(order.begin(), order.end(), 0u);
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t c) {
+        return (unsigned long long)b->hgraphs[a].E + b->hgraphs[a].V > (unsigned long long)b->hgraphs[c].E + b->hgraphs[c].V;
+    });
+    if (rc == SCC_OK &&
+        (cudaMemcpyAsync(b->dorder, order.data(), (size_t)n * 4, cudaMemcpyHostToDevice, b->stream) != cudaSuccess ||
+         cudaMemcpyAsync(b->dgraphs, b->hgraphs.data(), (size_t)n * sizeof(BatchGraph), cudaMemcpyHostToDevice, b->stream) != cudaSuccess ||
+         cudaStreamSynchronize(b->stream) != cudaSuccess))
+        rc = SCC_ERR_CUDA;
+    if (rc != SCC_OK) { cudaGetLastError(); batch_free(b); return rc; }
+    b->scratch_per_cta = carve_work(nullptr, b->maxV, b->maxE, true, nullptr);
+    rc = batch_reserve_scratch(b, b->threads, b->qcap);
+    if (rc != SCC_OK) { batch_free(b); return rc; }
+    *out = b;
+    return SCC_OK;
+}
+
+extern "C" int scc_batch_destroy(scc_batch *b)
+{
+    if (!b) return SCC_ERR_INVALID_ARG;
+    cudaSetDevice(b->ctx->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    batch_free(b);
+    return SCC_OK;
+}
+
+extern "C" int scc_batch_set_schedule(scc_batch *b, int threads, uint32_t qcap)
+{
+    if (!b || !(threads == 128 || threads == 256 || threads == 512 || threads == 1024) || qcap < 32 || qcap > 768)
+        return SCC_ERR_INVALID_ARG;
+    if (batch_smem(threads, qcap) > 200 * 1024) return SCC_ERR_INVALID_ARG;
+    cudaSetDevice(b->ctx->device);
+    int rc = batch_reserve_scratch(b, threads, qcap);
+    if (rc != SCC_OK) return rc;
+    b->threads = threads;
+    b->qcap = qcap;
+    return SCC_OK;
+}
+
+extern "C" int scc_batch_get_schedule(scc_batch *b, int *threads, uint32_t *qcap)
+{
+    if (!b) return SCC_ERR_INVALID_ARG;
+    if (threads) *threads = b->threads;
+    if (qcap) *qcap = b->qcap;
+    return SCC_OK;
+}
+
+static int lw_of(int algo, int w)
+{
+    if (algo != SCC_ALGO_WHONG && algo != SCC_ALGO_WSLOTA) return -1;
+    switch (w) {
+    case 1: return 0;
+    case 2: return 1;
+    case 4: return 2;
+    case 8: return 3;
+    case 16: return 4;
+    case 32: return 5;
+    default: return -2;
+    }
+}
+
+// Per-graph plain calls, one after the other: the baseline of the batched form.
+static int batch_run_sequential(scc_batch *b, int algo, uint32_t flags, int w, scc_stats *stats)
+{
+    for (uint32_t i = 0; i < b->n; i++) {
+        const BatchGraph &bg = b->hgraphs[i];
+        scc_csr_view v{bg.V, bg.E, b->dFr + bg.off_r, b->dFc + bg.off_c, b->dBr + bg.off_r, b->dBc + bg.off_c};
+        scc_stats st;
+        int rc = scc_run(b->ctx, &v, algo, (flags & ~SCC_FLAG_BATCH_SEQUENTIAL) | SCC_FLAG_DEVICE, w,
+                         b->dout + bg.off_out, &st, b->stream);
+        b->hres[i] = BatchRes{st.num_trim1, st.num_trim2, st.num_pivot, rc, st.error_where};
+        if (stats) stats->gpu_launches += st.gpu_launches;
+    }
+    cudaEventRecord(b->ev[1], b->stream);
+    cudaEventSynchronize(b->ev[1]);
+    if (stats) cudaEventElapsedTime(&stats->kernel_ms, b->ev[0], b->ev[1]);
+    return SCC_OK;
+}
+
+extern "C" int scc_batch_run(scc_batch *b, int algo, uint32_t flags, int warp_width, uint32_t *labels_out,
+                             scc_batch_result *results, scc_stats *stats)
+{
+    if (!b) return SCC_ERR_INVALID_ARG;
+    if (stats) memset(stats, 0, sizeof(*stats));
+    const bool hong = algo == SCC_ALGO_VHONG || algo == SCC_ALGO_WHONG;
+    if (!hong && algo != SCC_ALGO_VSLOTA && algo != SCC_ALGO_WSLOTA) return SCC_ERR_INVALID_ARG;
+    const int lw = lw_of(algo, warp_width);
+    if (lw == -2) return SCC_ERR_INVALID_ARG;
+    if (cudaSetDevice(b->ctx->device) != cudaSuccess) return SCC_ERR_NO_DEVICE;
+    cudaEventRecord(b->ev[0], b->stream);
+    if (flags & SCC_FLAG_BATCH_SEQUENTIAL) {
+        batch_run_sequential(b, algo, flags, warp_width, stats);
+    } else {
+        const uint32_t keyflags = flags & (SCC_FLAG_TRIM1 | SCC_FLAG_TRIM2);
+        if (!b->gexec || b->g_algo != algo || b->g_flags != keyflags || b->g_w != warp_width ||
+            b->g_threads != b->threads || b->g_qcap != b->qcap) {
+            if (b->gexec) { cudaGraphExecDestroy(b->gexec); b->gexec = nullptr; }
+            BatchParams p{b->dgraphs, b->dorder, b->n, b->dFr, b->dFc, b->dBr, b->dBc, 0u, b->dout, b->dres,
+                          b->scratch, (unsigned long long)b->scratch_per_cta, b->dnext, b->qcap, b->ctx->bu_k,
+                          (flags & SCC_FLAG_TRIM1) ? 1 : 0, (flags & SCC_FLAG_TRIM2) ? 1 : 0, lw,
+                          (unsigned long long)b->ctx->timeout_ms * 1000000ull};
+            void *fn = pick_batch_kernel(b->threads, hong);
+            void *args[] = {&p};
+            cudaGraph_t graph = nullptr;
+            if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+                cudaGetLastError();
+                return SCC_ERR_CUDA;
+            }
+            cudaMemsetAsync(b->dnext, 0, 4, b->stream);
+            cudaLaunchKernel(fn, dim3(b->ncta), dim3(b->threads), args, batch_smem(b->threads, b->qcap), b->stream);
+            if (cudaStreamEndCapture(b->stream, &graph) != cudaSuccess ||
+                cudaGraphInstantiate(&b->gexec, graph, 0) != cudaSuccess) {
+                if (graph) cudaGraphDestroy(graph);
+                cudaGetLastError();
+                return SCC_ERR_CUDA;
+            }
+            cudaGraphDestroy(graph);
+            b->g_algo = algo; b->g_flags = keyflags; b->g_w = warp_width;
+            b->g_threads = b->threads; b->g_qcap = b->qcap;
+        }
+        if (cudaGraphLaunch(b->gexec, b->stream) != cudaSuccess) { cudaGetLastError(); return SCC_ERR_CUDA; }
+        cudaEventRecord(b->ev[1], b->stream);
+        if (cudaMemcpyAsync(b->hres, b->dres, (size_t)b->n * sizeof(BatchRes), cudaMemcpyDeviceToHost, b->stream) != cudaSuccess) {
+            cudaGetLastError();
+            return SCC_ERR_CUDA;
+        }
+        if (stats) stats->gpu_launches = 1;
+    }
+    if (labels_out && b->sumV &&
+        cudaMemcpyAsync(labels_out, b->dout, b->sumV * 4, cudaMemcpyDeviceToHost, b->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return SCC_ERR_CUDA;
+    }
+    if (cudaStreamSynchronize(b->stream) != cudaSuccess) { cudaGetLastError(); return SCC_ERR_CUDA; }
+    int first_err = SCC_OK;
+    unsigned long long tot = 0;
+    for (uint32_t i = 0; i < b->n; i++) {
+        const BatchRes &r = b->hres[i];
+        if (results) results[i] = scc_batch_result{r.trim1 + r.trim2 + r.pivot, r.trim1, r.status, 0u};
+        if (r.status && first_err == SCC_OK) first_err = r.status;
+        tot += r.trim1 + r.trim2 + r.pivot;
+    }
+    if (stats) {
+        stats->num_sccs = tot;
+        stats->grid_blocks = (flags & SCC_FLAG_BATCH_SEQUENTIAL) ? 0u : b->ncta;
+        if (!(flags & SCC_FLAG_BATCH_SEQUENTIAL)) cudaEventElapsedTime(&stats->kernel_ms, b->ev[0], b->ev[1]);
+    }
+    return first_err;
+}
+
+// Picks the CTA size and staging slice by timing every candidate on the
+// batch itself (one untimed and two timed runs each).
+extern "C" int scc_batch_autotune(scc_batch *b, int algo, uint32_t flags, int warp_width, int *best_threads,
+                                  uint32_t *best_qcap, float *best_ms)
+{
+    if (!b) return SCC_ERR_INVALID_ARG;
+    const int cand_t[] = {128, 256, 512, 1024};
+    const uint32_t cand_q[] = {64, 256};
+    float best = 1e30f;
+    int bt = b->threads;
+    uint32_t bq = b->qcap;
+    for (int t : cand_t) {
+        for (uint32_t q : cand_q) {
+            if (scc_batch_set_schedule(b, t, q) != SCC_OK) continue;
+            scc_stats st;
+            int rc = scc_batch_run(b, algo, flags & ~SCC_FLAG_BATCH_SEQUENTIAL, warp_width, nullptr, nullptr, &st);
+            if (rc != SCC_OK && rc < SCC_ERR_OVERFLOW) return rc;
+            float ms = 0.f;
+            for (int rep = 0; rep < 2; rep++) {
+                scc_batch_run(b, algo, flags & ~SCC_FLAG_BATCH_SEQUENTIAL, warp_width, nullptr, nullptr, &st);
+                ms += st.kernel_ms;
+            }
+            if (ms < best) { best = ms; bt = t; bq = q; }
+        }
+    }
+    int rc = scc_batch_set_schedule(b, bt, bq);
+    if (best_threads) *best_threads = bt;
+    if (best_qcap) *best_qcap = bq;
+    if (best_ms) *best_ms = best / 2.f;
+    return rc;
+}
+
+extern "C" int scc_batch_info(scc_batch *b, uint64_t *num_vertices, uint64_t *num_edges, uint32_t *num_graphs)
+{
+    if (!b) return SCC_ERR_INVALID_ARG;
+    if (num_vertices) *num_vertices = b->sumV;
+    if (num_edges) *num_edges = b->sumE;
+    if (num_graphs) *num_graphs = b->n;
+    return SCC_OK;
+}

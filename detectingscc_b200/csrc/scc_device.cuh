@@ -103,8 +103,43 @@ struct Work {
     uint32_t bu_k;              // bottom-up BFS step when frontier edges > bu_k * scope vertices (0 = never)
 };
 
+// Carve the work arrays for a graph of V vertices and E edges out of `base`
+// (nullptr: only count).  Returns the bytes used.  Same layout on host and
+// device; used by the batched form, where every CTA re-carves its private
+// scratch for each graph it takes.
+__host__ __device__ inline size_t carve_work(char *base, uint32_t V, uint32_t E, bool hong, Work *w)
+{
+    const size_t n1 = (size_t)V + 1;
+    const size_t hcap = (size_t)E / CH + (size_t)E / HEAVY_T + 64;
+    const size_t va = (n1 * 4 + 255) / 256 * 256;       // one vertex array
+    const size_t ha = (hcap * 8 + 255) / 256 * 256;     // one chunk queue
+    const size_t pa = ((hong ? 4 * n1 + 8 : 1) * 8 + 255) / 256 * 256;
+    const size_t ca = (sizeof(Ctl) + 255) / 256 * 256;
+    if (w && base) {
+        w->st = (uint32_t *)(base);
+        w->label = (uint32_t *)(base + va);
+        w->stamp = (uint32_t *)(base + 2 * va);
+        w->smin = (uint32_t *)(base + 3 * va);
+        w->L[0] = (uint32_t *)(base + 4 * va);
+        w->L[1] = (uint32_t *)(base + 5 * va);
+        w->Q[0][0] = (uint32_t *)(base + 6 * va);
+        w->Q[0][1] = (uint32_t *)(base + 7 * va);
+        w->Q[1][0] = (uint32_t *)(base + 8 * va);
+        w->Q[1][1] = (uint32_t *)(base + 9 * va);
+        w->H[0][0] = (uint2 *)(base + 10 * va);
+        w->H[0][1] = (uint2 *)(base + 10 * va + ha);
+        w->H[1][0] = (uint2 *)(base + 10 * va + 2 * ha);
+        w->H[1][1] = (uint2 *)(base + 10 * va + 3 * ha);
+        w->hcap = (uint32_t)hcap;
+        w->pivkey = (unsigned long long *)(base + 10 * va + 4 * ha);
+        w->ctl = (Ctl *)(base + 10 * va + 4 * ha + pa);
+    }
+    return 10 * va + 4 * ha + pa + ca;
+}
+
 // Dynamic shared memory of the SCC kernels: BQ_HDR control words, then NBQ
-// staging queues, each split into one slice of qcap entries per warp.
+// staging queues, each split into one slice of qcap entries per warp of the
+// CTA: (BQ_HDR + NBQ * warps * qcap) words.
 constexpr unsigned NBQ = 2;
 constexpr unsigned BQ_WARPS = 32;                       // at most 1024 threads per CTA
 constexpr unsigned BQ_CNT = 16;                         // per-warp fill counts [NBQ][BQ_WARPS]
@@ -284,7 +319,7 @@ __device__ __forceinline__ void bq_push(unsigned qi, bool pred, uint32_t val, ui
     const unsigned m = __ballot_sync(FULL, pred);
     if (m == 0u) return;
     const unsigned lane = lane_id(), wi = threadIdx.x >> 5;
-    uint32_t *slice = &sccb_dsmem[BQ_HDR + (qi * BQ_WARPS + wi) * qcap];
+    uint32_t *slice = &sccb_dsmem[BQ_HDR + (qi * (blockDim.x >> 5) + wi) * qcap];
     unsigned *wc = &sccb_dsmem[BQ_CNT + qi * BQ_WARPS + wi];
     unsigned cnt = *wc;
     const unsigned n = __popc(m);
@@ -339,7 +374,7 @@ __device__ __forceinline__ void bq_flush(unsigned nq, uint32_t qcap, uint32_t *g
         uint32_t *gq = qi ? gq1 : gq0;
         const unsigned cnt = sccb_dsmem[BQ_CNT + qi * BQ_WARPS + wi];
         const unsigned base = sccb_dsmem[8 + qi] + sccb_dsmem[BQ_PRE + qi * BQ_WARPS + wi];
-        const uint32_t *slice = &sccb_dsmem[BQ_HDR + (qi * BQ_WARPS + wi) * qcap];
+        const uint32_t *slice = &sccb_dsmem[BQ_HDR + (qi * nw + wi) * qcap];
         for (unsigned i = lane_id(); i < cnt; i += 32u) {
             if (base + i < gcap) gq[base + i] = slice[i];
             else set_error(ctl, E_OVERFLOW, 3);

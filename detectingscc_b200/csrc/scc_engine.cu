@@ -36,7 +36,10 @@ struct Params {
 constexpr int GRID_THREADS = 1024;
 constexpr int BLOCK_THREADS = 1024;
 
-static size_t dyn_smem_bytes(uint32_t qcap) { return (BQ_HDR + NBQ * BQ_WARPS * (size_t)qcap) * sizeof(uint32_t); }
+static size_t dyn_smem_bytes(uint32_t qcap, int threads = 1024)
+{
+    return (BQ_HDR + NBQ * (size_t)(threads / 32) * qcap) * sizeof(uint32_t);
+}
 
 template <bool INSTR, bool HONG>
 __global__ void __launch_bounds__(GRID_THREADS, 1) k_scc_grid(Params p)

@@ -51,6 +51,7 @@ typedef enum {
 #define SCC_FLAG_INSTRUMENT 0x8u     /* count adjacency entries / vertex visits (slower) */
 #define SCC_FLAG_FORCE_GRID 0x10u    /* always use the whole-GPU persistent launch */
 #define SCC_FLAG_FORCE_BLOCK 0x20u   /* always use the single-CTA launch */
+#define SCC_FLAG_BATCH_SEQUENTIAL 0x40u /* scc_batch_run: one plain scc_run per graph (the baseline) */
 
 #define SCC_MAX_VERTICES 268435454u  /* 2^28 - 2 */
 #define SCC_MAX_EDGES 4294967040u     /* 2^32 - 256 */
@@ -185,22 +186,36 @@ int scc_reference_call(int algo, uint32_t CSize, uint32_t RSize, const uint32_t 
                        uint64_t *num_sccs_out);
 
 /* ---- batched form: many independent graphs, one persistent launch ------ */
+/* No counterpart in the reference, which runs one graph per process.  The
+ * graphs are uploaded once (host CSR views) into one device arena and stay
+ * resident until scc_batch_destroy.  scc_batch_run runs all of them in one
+ * launch (captured once into a CUDA graph and replayed): every CTA takes the
+ * next graph, largest first, and runs the same driver code as scc_run on a
+ * private scratch slice.  With SCC_FLAG_BATCH_SEQUENTIAL it instead calls
+ * scc_run once per graph, in order, on one stream (the baseline). */
 typedef struct scc_batch scc_batch;
 
-/* Upload `n` graphs (host CSR views) into one device arena.  The graphs stay
- * resident until scc_batch_destroy. */
-int scc_batch_create(scc_context *ctx, const scc_csr_view *graphs, uint32_t n, scc_batch **out);
-/* Run all graphs of the batch; labels_out (host) receives the concatenation
- * of every graph's V labels in batch order, counts_out (host, optional)
- * n entries of scc_batch_result. */
 typedef struct {
     uint64_t num_sccs;
     uint64_t num_trim1;
-    int32_t status;
+    int32_t status;     /* SCC_OK or the graph's own error; other graphs are unaffected */
     uint32_t reserved;
 } scc_batch_result;
+
+int scc_batch_create(scc_context *ctx, const scc_csr_view *graphs, uint32_t n, scc_batch **out);
+/* labels_out (host, optional): the concatenation of every graph's V labels in
+ * batch order; results (host, optional): n entries.  Returns SCC_OK or the
+ * first graph error. */
 int scc_batch_run(scc_batch *b, int algo, uint32_t flags, int warp_width, uint32_t *labels_out,
                   scc_batch_result *results, scc_stats *stats);
+/* Schedule of the batched launch: CTA size (128, 256, 512, 1024) and the
+ * per-warp staging slice (32..768 entries). */
+int scc_batch_set_schedule(scc_batch *b, int threads, uint32_t qcap);
+int scc_batch_get_schedule(scc_batch *b, int *threads, uint32_t *qcap);
+/* Times every candidate schedule on the batch and keeps the fastest. */
+int scc_batch_autotune(scc_batch *b, int algo, uint32_t flags, int warp_width, int *best_threads,
+                       uint32_t *best_qcap, float *best_ms);
+int scc_batch_info(scc_batch *b, uint64_t *num_vertices, uint64_t *num_edges, uint32_t *num_graphs);
 int scc_batch_destroy(scc_batch *b);
 
 #ifdef __cplusplus
