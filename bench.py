@@ -49,6 +49,10 @@ CONFIGS = {
     "cfg3": dict(algo="y", t1=True, t2=True, warp=8,
                  desc="wSlota -w 8 -p 1 -q 1 on a 4096x4096 grid, 70% bidirectional pairs, 30% one "
                       "random orientation, +0.1% uniform long-range arcs"),
+    "cfg4": dict(algo="h", t1=True, t2=True, warp=1,
+                 desc="batched: 4,096 graphs, V log-uniform in [64, 65536], mean out-degree U[4, 16], half "
+                      "Erdos-Renyi, half planted-SCC chains; vSlota -p 1 -q 1; one launch under a CUDA graph "
+                      "vs per-graph plain launches"),
 }
 
 
@@ -289,6 +293,98 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def _batch_graphs(n_graphs: int, seed: int = 1):
+    import concurrent.futures as cf
+
+    import detectingscc_b200 as scc
+    from detectingscc_b200 import graphs
+    arcs = graphs.batch_mix(n_graphs, seed=seed)
+    with cf.ThreadPoolExecutor(os.cpu_count() or 1) as ex:   # the CSR builder releases the GIL
+        return list(ex.map(lambda a: scc.graph_from_arcs(*a), arcs))
+
+
+def run_batch(args):
+    """cfg4: graphs/s of the batched launch vs per-graph plain launches."""
+    import torch
+
+    import detectingscc_b200 as scc
+    world, rank, local = _dist_init()
+    torch.cuda.set_device(local)
+    cfg = CONFIGS["cfg4"]
+    n_graphs = args.scale or 4096
+    gs = _batch_graphs(n_graphs, seed=1 + rank)
+    eng = scc.Engine(local)
+    b = scc.Batch(eng, gs)
+    t_ins = time.perf_counter()
+    best_t, best_q, _ = b.autotune(algo=cfg["algo"], t1=cfg["t1"], t2=cfg["t2"], warp=cfg["warp"])
+    t_tune = time.perf_counter() - t_ins
+    for _ in range(args.warmup):
+        b.run(algo=cfg["algo"], t1=cfg["t1"], t2=cfg["t2"], warp=cfg["warp"], labels=False)
+    clocks = ClockSampler(local)
+    _barrier(world)
+    clocks.start()
+    ms = []
+    for _ in range(args.steps):
+        _, res, st = b.run(algo=cfg["algo"], t1=cfg["t1"], t2=cfg["t2"], warp=cfg["warp"], labels=False)
+        ms.append(st["kernel_ms"])
+    _barrier(world)
+    clk = clocks.stop()
+    t_batch = _max_over_ranks(sum(ms) / len(ms), world)
+    # per-graph plain launches of the same engine (sequential, state resident)
+    seq = []
+    for _ in range(max(1, min(3, args.steps))):
+        _, res_s, st_s = b.run(algo=cfg["algo"], t1=cfg["t1"], t2=cfg["t2"], warp=cfg["warp"], labels=False,
+                               sequential=True)
+        seq.append(st_s["kernel_ms"])
+    t_seq = _max_over_ranks(sum(seq) / len(seq), world)
+    assert [r[0] for r in res] == [r[0] for r in res_s]
+    # end to end: upload every graph from host memory, run, read all labels back
+    e2e = []
+    hlab = np.zeros(b.total_vertices, dtype=np.uint32)
+    for _ in range(max(1, min(3, args.steps))):
+        t0 = time.perf_counter()
+        b2 = scc.Batch(eng, gs)
+        b2.set_schedule(best_t, best_q)
+        b2.run(algo=cfg["algo"], t1=cfg["t1"], t2=cfg["t2"], warp=cfg["warp"], out=hlab)
+        e2e.append(time.perf_counter() - t0)
+        b2.close()
+    t_e2e = _max_over_ranks(sum(e2e) / len(e2e), world)
+    sumE = b.total_edges
+    out = {
+        "metric": "batched SCC graphs/s (cfg4)", "value": round(world * n_graphs / (t_batch * 1e-3), 1),
+        "unit": "graphs/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(t_batch, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32", "data": "synthetic (seeded generator, no dataset)",
+        "config": {"workload": f"cfg4: {cfg['desc']}", "graphs": n_graphs, "sum_V": b.total_vertices,
+                   "sum_E": sumE, "seed": 1, "schedule": {"threads": best_t, "qcap": best_q,
+                                                          "autotune_s": round(t_tune, 2)},
+                   "l2": "inputs larger than L2", "parallelism": "graphs sharded per rank" if world > 1 else "single GPU"},
+        "per_graph_plain": {"ms_per_batch": round(t_seq, 3), "graphs_per_s": round(world * n_graphs / (t_seq * 1e-3), 1)},
+        "batched_over_plain": round(t_seq / t_batch, 2),
+        "Medges_per_s": round(world * sumE / (t_batch * 1e-3) / 1e6, 1),
+        "e2e": {"value": round(world * n_graphs / t_e2e, 1), "unit": "graphs/s", "ms_per_step": round(t_e2e * 1e3, 2),
+                "h2d_bytes_per_step": int(sum(g.nbytes for g in gs)), "d2h_bytes_per_step": int(4 * b.total_vertices)},
+        "gpu_launches": int(args.steps), "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import concurrent.futures as cf
+
+        from oracle import oracle
+        cores = os.cpu_count() or 1
+        sample = gs[: max(64, n_graphs // 8)]
+        t0 = time.perf_counter()
+        with cf.ThreadPoolExecutor(cores) as ex:
+            list(ex.map(lambda g: oracle.tarjan(g.V, g.Fr, g.Fc), sample))
+        t_cpu = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": round(len(sample) / t_cpu, 1), "unit": "graphs/s", "cores": cores,
+                               "kind": "port", "sample": f"first {len(sample)} graphs of the mix, iterative "
+                                                         f"Tarjan per graph on a {cores}-thread pool"}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    b.close()
+    eng.close()
+
+
 def run_reference(args):
     world, rank, local = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), \
         int(os.environ.get("LOCAL_RANK", "0"))
@@ -299,6 +395,29 @@ def run_reference(args):
     from detectingscc_b200 import graphs
     from oracle import oracle
     cfg = CONFIGS[args.config]
+    if args.config == "cfg4":
+        import concurrent.futures as cf
+        gs = _batch_graphs(args.scale or 4096, seed=1)
+        cores = os.cpu_count() or 1
+        sample = gs[: max(64, len(gs) // 8)]
+        times = []
+        for i in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            with cf.ThreadPoolExecutor(cores) as ex:
+                list(ex.map(lambda g: oracle.tarjan(g.V, g.Fr, g.Fc), sample))
+            if i >= args.warmup:
+                times.append(time.perf_counter() - t0)
+        v = round(len(sample) / (sum(times) / len(times)), 1)
+        print(json.dumps({"impl": "reference", "metric": "batched SCC graphs/s (cfg4)", "value": v, "unit": "graphs/s",
+                          "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+                          "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+                          "config": {"workload": f"cfg4: {cfg['desc']}", "graphs": len(gs)},
+                          "cpu_baseline": {"value": v, "unit": "graphs/s", "cores": cores, "kind": "port",
+                                           "sample": f"first {len(sample)} graphs per step, Tarjan per graph on a "
+                                                     f"{cores}-thread pool (the reference has no CPU SCC path)"},
+                          "e2e": {"value": v, "unit": "graphs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+              flush=True)
+        return
     dev = torch.device("cuda", local) if torch.cuda.is_available() else torch.device("cpu")
     V, s, d = _gen_graph(args.config, args.scale, dev)
     Fr, Fc, Br, Bc = (t.cpu().numpy().view(np.uint32) for t in graphs.csr_from_arcs_torch(V, s, d))
@@ -377,6 +496,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.config == "cfg4":
+        run_batch(args)
     else:
         run_ours(args)
 

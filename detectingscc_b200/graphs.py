@@ -145,30 +145,34 @@ def _planted_chain(V: int, deg: float, rng: np.random.Generator) -> Tuple[np.nda
     """k strongly connected blocks (cycle + chords) linked acyclically."""
     k = int(rng.integers(2, max(3, V // 8)))
     cuts = np.sort(rng.choice(np.arange(1, V), size=min(k - 1, V - 1), replace=False))
-    bounds = np.concatenate([[0], cuts, [V]])
-    perm = rng.permutation(V) + 1
-    srcs, dsts = [], []
-    for i in range(len(bounds) - 1):
-        blk = perm[bounds[i]:bounds[i + 1]]
-        if len(blk) > 1:
-            srcs.append(blk)
-            dsts.append(np.roll(blk, -1))
-            nch = int(len(blk) * max(deg - 2.0, 0.0) * 0.5)
-            if nch:
-                srcs.append(rng.choice(blk, nch))
-                dsts.append(rng.choice(blk, nch))
-    # acyclic links: from block i to a later block
+    bounds = np.concatenate([[0], cuts, [V]]).astype(np.int64)
+    nb = len(bounds) - 1
+    perm = rng.permutation(V).astype(np.int64) + 1
+    start = np.repeat(bounds[:-1], np.diff(bounds))          # block start of every position
+    end = np.repeat(bounds[1:], np.diff(bounds))
+    pos = np.arange(V, dtype=np.int64)
+    nxt = np.where(pos + 1 < end, pos + 1, start)             # cycle inside each block
+    multi = (end - start) > 1
+    srcs, dsts = [perm[pos[multi]]], [perm[nxt[multi]]]
+    # chords inside blocks: a random position, then a random position of the same block
+    n_ch = int(V * max(deg - 2.0, 0.0) * 0.5)
+    if n_ch:
+        p1 = rng.integers(0, V, n_ch)
+        p2 = start[p1] + (rng.random(n_ch) * (end[p1] - start[p1])).astype(np.int64)
+        srcs.append(perm[p1])
+        dsts.append(perm[p2])
+    # acyclic links from a block to a later block
     n_links = int(V * min(deg, 4.0) * 0.5)
-    bi = rng.integers(0, len(bounds) - 1, n_links)
-    bj = rng.integers(0, len(bounds) - 1, n_links)
+    bi = rng.integers(0, nb, n_links)
+    bj = rng.integers(0, nb, n_links)
     lo, hi = np.minimum(bi, bj), np.maximum(bi, bj)
     ok = lo < hi
     lo, hi = lo[ok], hi[ok]
-    su = perm[(bounds[lo] + (rng.random(len(lo)) * (bounds[lo + 1] - bounds[lo])).astype(np.int64))]
-    sv = perm[(bounds[hi] + (rng.random(len(hi)) * (bounds[hi + 1] - bounds[hi])).astype(np.int64))]
+    su = perm[bounds[lo] + (rng.random(len(lo)) * (bounds[lo + 1] - bounds[lo])).astype(np.int64)]
+    sv = perm[bounds[hi] + (rng.random(len(hi)) * (bounds[hi + 1] - bounds[hi])).astype(np.int64)]
     srcs.append(su)
     dsts.append(sv)
-    return np.concatenate(srcs).astype(np.int64), np.concatenate(dsts).astype(np.int64)
+    return np.concatenate(srcs), np.concatenate(dsts)
 
 
 def batch_mix(n_graphs: int = 4096, vmin: int = 64, vmax: int = 65536, dmin: float = 4.0,
