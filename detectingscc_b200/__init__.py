@@ -7,9 +7,9 @@ Python host mirror.  There is no CPU fallback: without the library every
 call raises ``NativeLibraryError``.
 """
 from ._native import NativeLibraryError, SCCError  # noqa: F401
-from .api import (ALGOS, Batch, Engine, Graph, Result, graph_from_arcs, load_graph,  # noqa: F401
+from .api import (ALGOS, Batch, Engine, Graph, Result, Server, graph_from_arcs, load_graph,  # noqa: F401
                   loadFullGraph, save_binary, vHong, vSlota, wHong, wSlota)
 
-__all__ = ["Batch", "Engine", "Graph", "Result", "graph_from_arcs", "load_graph", "loadFullGraph",
+__all__ = ["Batch", "Engine", "Server", "Graph", "Result", "graph_from_arcs", "load_graph", "loadFullGraph",
            "save_binary", "vHong", "vSlota", "wHong", "wSlota", "NativeLibraryError", "SCCError",
            "ALGOS"]

@@ -45,6 +45,18 @@ class HostGraph(ctypes.Structure):
                 ("Pr", u32p)]
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("budget_bytes", u64), ("lanes", u32), ("max_graphs_per_batch", u32), ("large_vertices", u32),
+                ("batch_threads", ctypes.c_int32), ("qcap", u32), ("algo", ctypes.c_int32), ("flags", u32),
+                ("warp_width", ctypes.c_int32)]
+
+
+class ServerResult(ctypes.Structure):
+    _fields_ = [("ticket", u64), ("status", ctypes.c_int32), ("num_vertices", u32), ("num_sccs", u64),
+                ("num_trim1", u64), ("latency_ms", ctypes.c_double), ("queue_ms", ctypes.c_double),
+                ("lane", ctypes.c_int32), ("reserved", u32)]
+
+
 class BatchResult(ctypes.Structure):
     _fields_ = [("num_sccs", u64), ("num_trim1", u64), ("status", ctypes.c_int32), ("reserved", u32)]
 
@@ -70,7 +82,8 @@ C_SYMBOLS = ["scc_create", "scc_destroy", "scc_run", "scc_set_tuning", "scc_stat
              "scc_version", "scc_get_trace", "scc_load_graph", "scc_save_binary", "scc_graph_from_arcs",
              "scc_free_host_graph", "scc_reference_call", "scc_batch_create", "scc_batch_run",
              "scc_batch_destroy", "scc_run_noalloc", "scc_batch_set_schedule", "scc_batch_get_schedule",
-             "scc_batch_autotune", "scc_batch_info"]
+             "scc_batch_autotune", "scc_batch_info", "scc_server_create", "scc_server_submit",
+             "scc_server_poll", "scc_server_info", "scc_server_destroy"]
 CXX_SYMBOLS = ["_Z5vHongjjPjS_S_S_bb", "_Z6vSlotajjPjS_S_S_bb", "_Z5wHongjjPjS_S_S_bbi",
                "_Z6wSlotajjPjS_S_S_bbi", "_Z13loadFullGraphPKcPjS1_PS1_S2_S2_S2_S2_"]
 
@@ -124,6 +137,11 @@ def lib():
     L.scc_batch_info.argtypes = [vp, ctypes.POINTER(u64), ctypes.POINTER(u64), ctypes.POINTER(u32)]
     L.scc_run_noalloc.argtypes = [ctypes.POINTER(CsrView), ctypes.c_int, u32, ctypes.c_int, vp,
                                   ctypes.POINTER(Stats), vp]
+    L.scc_server_create.argtypes = [ctypes.c_int, ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]
+    L.scc_server_submit.argtypes = [vp, ctypes.POINTER(CsrView), vp, ctypes.POINTER(u64)]
+    L.scc_server_poll.argtypes = [vp, ctypes.POINTER(ServerResult), u32, ctypes.POINTER(u32), ctypes.c_int]
+    L.scc_server_info.argtypes = [vp, ctypes.POINTER(u64), ctypes.POINTER(u64), ctypes.POINTER(u64), ctypes.POINTER(u64)]
+    L.scc_server_destroy.argtypes = [vp]
     L.scc_get_trace.argtypes = [vp, ctypes.POINTER(u64), u32, ctypes.POINTER(u32), ctypes.POINTER(u64)]
     _lib = L
     return L

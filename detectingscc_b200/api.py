@@ -233,6 +233,63 @@ class Batch:
         return labels[self.offsets[i]:self.offsets[i + 1]]
 
 
+class Server:
+    """Request server: continuous batching under a device-memory budget.
+
+    submit() queues one host graph and the host array its labels go to;
+    both must stay alive until the request's result has been polled.
+    """
+
+    def __init__(self, device: int = 0, algo="h", t1=True, t2=True, warp=1, budget_bytes: int = 0, lanes: int = 0,
+                 max_graphs_per_batch: int = 0, large_vertices: int = 0, batch_threads: int = 0, qcap: int = 0):
+        self._lib = N.lib()
+        cfg = N.ServerConfig(int(budget_bytes), int(lanes), int(max_graphs_per_batch), int(large_vertices),
+                             int(batch_threads), int(qcap), _algo_code(algo),
+                             (N.FLAG_TRIM1 if t1 else 0) | (N.FLAG_TRIM2 if t2 else 0), int(warp))
+        h = ctypes.c_void_p()
+        N.check(self._lib.scc_server_create(int(device), ctypes.byref(cfg), ctypes.byref(h)), "scc_server_create")
+        self._h = h
+        self._live = {}   # ticket -> (graph, labels) kept alive until polled
+
+    def submit(self, g: Graph, out: Optional[np.ndarray] = None) -> int:
+        if out is None:
+            out = np.zeros(max(g.V, 1), dtype=np.uint32)
+        view = N.CsrView(g.V, g.E, _ptr(g.Fr), _ptr(g.Fc), _ptr(g.Br), _ptr(g.Bc))
+        t = ctypes.c_uint64(0)
+        N.check(self._lib.scc_server_submit(self._h, ctypes.byref(view), _ptr(out), ctypes.byref(t)), "scc_server_submit")
+        self._live[t.value] = (g, out)
+        return t.value
+
+    def poll(self, max_results: int = 1024, wait_ms: int = 0):
+        """Finished requests: list of dicts with ticket, status, counts, latency and the labels array."""
+        buf = (N.ServerResult * max_results)()
+        n = ctypes.c_uint32(0)
+        N.check(self._lib.scc_server_poll(self._h, buf, max_results, ctypes.byref(n), int(wait_ms)))
+        out = []
+        for r in buf[:n.value]:
+            g, lab = self._live.pop(r.ticket, (None, None))
+            out.append({"ticket": r.ticket, "status": r.status, "num_sccs": r.num_sccs, "num_trim1": r.num_trim1,
+                        "latency_ms": r.latency_ms, "queue_ms": r.queue_ms, "lane": r.lane,
+                        "labels": lab[:g.V] if g is not None else None})
+        return out
+
+    def info(self):
+        a, b, c, d = (ctypes.c_uint64(0) for _ in range(4))
+        N.check(self._lib.scc_server_info(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(d)))
+        return {"pending": a.value, "completed": b.value, "held_bytes": c.value, "rejected": d.value}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.scc_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 # ----------------------------------------------------------------------
 # graph files
 # ----------------------------------------------------------------------

@@ -30,10 +30,10 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-Wall", "-I/usr/local/cuda/include"]
 
-CU_SOURCES = ["scc_engine.cu", "scc_batch.cu", "scc_noalloc.cu"]
+CU_SOURCES = ["scc_engine.cu", "scc_batch.cu", "scc_noalloc.cu", "scc_serve.cu"]
 CXX_LIB_SOURCES = ["gtgraph_load.cpp", "scc_compat.cpp"]
 CXX_CLI_SOURCES = ["scc_cli.cpp"]
-HEADERS = ["scc_device.cuh", "scc_phases.cuh", "scc_internal.h", "scc_host.h"]
+HEADERS = ["scc_device.cuh", "scc_phases.cuh", "scc_internal.h", "scc_host.h", "scc_batch_internal.h"]
 
 
 def _newer(target: str, deps) -> bool:
@@ -73,10 +73,10 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> str:
             lib_objs.append(o)
     all_lib = objs + lib_objs
     if force or _newer(LIB, all_lib):
-        _run([NVCC] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-o", LIB] + all_lib)
+        _run([NVCC] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-o", LIB] + all_lib + ["-lpthread"])
     cli_obj = os.path.join(BUILD, "scc_cli.cpp.o")
     if force or _newer(CLI, all_lib + [cli_obj]):
-        _run([NVCC] + ARCH + ["-o", CLI, cli_obj] + all_lib)
+        _run([NVCC] + ARCH + ["-o", CLI, cli_obj] + all_lib + ["-lpthread"])
     return LIB
 
 

@@ -29,35 +29,9 @@
 
 using namespace sccb;
 
+#include "scc_batch_internal.h"
+
 namespace {
-
-struct BatchGraph {
-    uint32_t V, E;
-    unsigned long long off_r;   // into the packed Fr / Br arrays (V+2 entries per graph)
-    unsigned long long off_c;   // into the packed Fc / Bc arrays
-    unsigned long long off_out; // into the packed label output (V entries per graph)
-};
-
-struct BatchRes {
-    unsigned long long trim1, trim2, pivot;
-    int status, where;
-};
-
-struct BatchParams {
-    const BatchGraph *graphs;
-    const uint32_t *order;
-    uint32_t n;
-    const uint32_t *Fr, *Fc, *Br, *Bc;
-    uint32_t vec;
-    uint32_t *out;
-    BatchRes *res;
-    char *scratch;
-    unsigned long long scratch_per_cta;
-    unsigned *next;
-    uint32_t qcap, bu_k;
-    int t1, t2, lw;
-    unsigned long long timeout_ns;
-};
 
 template <int THREADS, bool HONG>
 __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_scc_batch(BatchParams p)
@@ -133,6 +107,40 @@ void *pick_batch_kernel(int threads, bool hong)
 size_t batch_smem(int threads, uint32_t qcap) { return (BQ_HDR + NBQ * (size_t)(threads / 32) * qcap) * 4; }
 
 }  // namespace
+
+size_t sccb_batch_smem(int threads, uint32_t qcap) { return batch_smem(threads, qcap); }
+
+int sccb_batch_ctas(int threads, uint32_t qcap, int nsm, uint32_t *out)
+{
+    const size_t smem = batch_smem(threads, qcap);
+    for (int h = 0; h < 2; h++)
+        if (cudaFuncSetAttribute(pick_batch_kernel(threads, h != 0), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem) != cudaSuccess) {
+            cudaGetLastError();
+            return SCC_ERR_CUDA;
+        }
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pick_batch_kernel(threads, true), threads, smem) !=
+            cudaSuccess || occ <= 0) {
+        cudaGetLastError();
+        return SCC_ERR_CUDA;
+    }
+    *out = (uint32_t)(occ * nsm);
+    return SCC_OK;
+}
+
+int sccb_batch_launch(const BatchParams &p, int threads, bool hong, uint32_t ncta, cudaStream_t st)
+{
+    BatchParams q = p;
+    void *args[] = {&q};
+    cudaError_t e = cudaLaunchKernel(pick_batch_kernel(threads, hong), dim3(ncta), dim3(threads), args,
+                                     batch_smem(threads, p.qcap), st);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return SCC_ERR_CUDA;
+    }
+    return SCC_OK;
+}
 
 struct scc_batch {
     scc_context *ctx = nullptr;

@@ -156,6 +156,51 @@ const char *scc_version(void);
 int scc_run_noalloc(const scc_csr_view *g, int algo, uint32_t flags, int warp_width, uint32_t *labels_out,
                     scc_stats *stats, void *stream);
 
+/* ---- serving form: continuous batching under a device-memory budget ---- */
+/* No counterpart in the reference.  A request is one host CSR plus a host
+ * buffer for its V labels; both stay owned by the caller and must remain
+ * valid until the request's result is polled.  `lanes` worker threads, each
+ * with its own stream, take whatever has arrived: a graph above
+ * large_vertices alone on the whole-GPU path, otherwise every waiting small
+ * graph (up to max_graphs_per_batch) in one batched launch.  Lanes run
+ * concurrently, so later arrivals overlap on the device with earlier work.
+ * All device memory the server holds stays within budget_bytes; a request
+ * that cannot fit even alone gets SCC_ERR_BUDGET.  Zero fields take the
+ * defaults shown. */
+typedef struct {
+    uint64_t budget_bytes;          /* 120e9 */
+    uint32_t lanes;                 /* 4 */
+    uint32_t max_graphs_per_batch;  /* 512 */
+    uint32_t large_vertices;        /* 65536 */
+    int32_t batch_threads;          /* 256 (128, 256, 512, 1024) */
+    uint32_t qcap;                  /* 128 */
+    int32_t algo;                   /* SCC_ALGO_VSLOTA */
+    uint32_t flags;                 /* SCC_FLAG_TRIM1 | SCC_FLAG_TRIM2 as wanted (host inputs only) */
+    int32_t warp_width;             /* 1 */
+} scc_server_config;
+
+typedef struct {
+    uint64_t ticket;
+    int32_t status;
+    uint32_t num_vertices;
+    uint64_t num_sccs;
+    uint64_t num_trim1;
+    double latency_ms;              /* submit -> labels in the caller's buffer */
+    double queue_ms;                /* submit -> a lane started it */
+    int32_t lane;
+    uint32_t reserved;
+} scc_server_result;
+
+typedef struct scc_server scc_server;
+int scc_server_create(int device, const scc_server_config *cfg, scc_server **out);
+/* Thread-safe.  *ticket identifies the request in its result. */
+int scc_server_submit(scc_server *s, const scc_csr_view *host_graph, uint32_t *labels_out, uint64_t *ticket);
+/* Returns up to cap finished results (waits up to wait_ms for one). */
+int scc_server_poll(scc_server *s, scc_server_result *out, uint32_t cap, uint32_t *n, int wait_ms);
+int scc_server_info(scc_server *s, uint64_t *pending, uint64_t *completed, uint64_t *held_bytes, uint64_t *rejected);
+/* Finishes every submitted request, then frees everything. */
+int scc_server_destroy(scc_server *s);
+
 /* ---- graph files ------------------------------------------------------ */
 /* A host CSR owned by the library (arrays allocated with new[], as the
  * reference loader does, load.cpp:52-115). */

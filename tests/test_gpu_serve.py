@@ -1,0 +1,109 @@
+"""Serving form: every result is the same alone and in the mix (integer
+labels, tolerance 0), requests arriving while others run are served, and
+the memory budget is enforced."""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+import detectingscc_b200 as scc
+
+pytestmark = pytest.mark.gpu
+
+
+def _pool(seed=11):
+    from detectingscc_b200 import graphs
+    small = [scc.graph_from_arcs(V, s, d) for V, s, d in graphs.batch_mix(48, vmin=16, vmax=4000, seed=seed)]
+    V, s, d = graphs.rmat(16, seed=seed)
+    large = graphs.to_graph(V, s, d)     # above large_vertices below: whole-GPU path
+    return small, large
+
+
+def test_results_same_alone_and_in_the_mix(oracle_lib):
+    small, large = _pool()
+    eng = scc.Engine(0)
+    alone = [eng.run(g, algo="h").labels.copy() for g in small + [large]]
+    eng.close()
+    srv = scc.Server(0, algo="h", lanes=3, large_vertices=32768, max_graphs_per_batch=16)
+    try:
+        mix = []
+        rng = np.random.default_rng(0)
+        order = rng.permutation(len(small) * 3 + 4)
+        tickets = {}
+        for k in order:
+            g = large if k >= len(small) * 3 else small[k % len(small)]
+            idx = len(small) if g is large else k % len(small)
+            tickets[srv.submit(g)] = idx
+            if k % 7 == 0:
+                time.sleep(0.001)   # arrivals spread over time, overlapping running work
+        got = 0
+        t0 = time.time()
+        while got < len(tickets) and time.time() - t0 < 120:
+            for r in srv.poll(256, wait_ms=200):
+                assert r["status"] == 0, r
+                i = tickets[r["ticket"]]
+                assert np.array_equal(r["labels"], alone[i]), i
+                got += 1
+                mix.append(r)
+        assert got == len(tickets)
+        assert max(r["lane"] for r in mix) >= 1          # more than one lane worked
+        # labels also equal Tarjan
+        lab, _ = oracle_lib.tarjan(large.V, large.Fr, large.Fc)
+        assert np.array_equal(alone[-1], lab[1:])
+    finally:
+        srv.close()
+
+
+def test_budget_rejects_oversize_request():
+    small, large = _pool(seed=3)
+    budget = 8 << 20
+    srv = scc.Server(0, algo="g", lanes=2, budget_bytes=budget, large_vertices=32768)
+    try:
+        t_big = srv.submit(large)          # the whole-GPU path needs more than 8 MiB for this graph
+        ts = [srv.submit(g) for g in small[:10]]
+        res = {}
+        t0 = time.time()
+        while len(res) < 11 and time.time() - t0 < 60:
+            for r in srv.poll(64, wait_ms=200):
+                res[r["ticket"]] = r
+        assert len(res) == 11
+        for t in ts:
+            assert res[t]["status"] == 0
+        info = srv.info()
+        assert info["held_bytes"] <= budget
+        assert res[t_big]["status"] == 6           # SCC_ERR_BUDGET
+        assert info["rejected"] == 1
+    finally:
+        srv.close()
+
+
+def test_concurrent_submitters():
+    small, _ = _pool(seed=5)
+    eng = scc.Engine(0)
+    alone = [eng.run(g, algo="g").labels.copy() for g in small]
+    eng.close()
+    srv = scc.Server(0, algo="g", lanes=4)
+    results = {}
+    lock = threading.Lock()
+
+    def producer(off):
+        for i in range(off, len(small), 4):
+            t = srv.submit(small[i])
+            with lock:
+                results[t] = i
+
+    try:
+        th = [threading.Thread(target=producer, args=(o,)) for o in range(4)]
+        [t.start() for t in th]
+        [t.join() for t in th]
+        got = 0
+        t0 = time.time()
+        while got < len(small) and time.time() - t0 < 60:
+            for r in srv.poll(64, wait_ms=200):
+                assert r["status"] == 0
+                assert np.array_equal(r["labels"], alone[results[r["ticket"]]])
+                got += 1
+        assert got == len(small)
+    finally:
+        srv.close()
