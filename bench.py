@@ -49,10 +49,14 @@ CONFIGS = {
     "cfg3": dict(algo="y", t1=True, t2=True, warp=8,
                  desc="wSlota -w 8 -p 1 -q 1 on a 4096x4096 grid, 70% bidirectional pairs, 30% one "
                       "random orientation, +0.1% uniform long-range arcs"),
-    "cfg4": dict(algo="h", t1=True, t2=True, warp=1,
+    "cfg4": dict(algo="g", t1=True, t2=True, warp=1,
                  desc="batched: 4,096 graphs, V log-uniform in [64, 65536], mean out-degree U[4, 16], half "
-                      "Erdos-Renyi, half planted-SCC chains; vSlota -p 1 -q 1; one launch under a CUDA graph "
+                      "Erdos-Renyi, half planted-SCC chains; vHong -p 1 -q 1; one launch under a CUDA graph "
                       "vs per-graph plain launches"),
+    "cfg5": dict(algo="g", t1=True, t2=True, warp=1,
+                 desc="serving: Poisson arrivals at 2,000 req/s, 95% graphs from the cfg4 distribution, 5% R-MAT "
+                      "scale 20 (1,048,576 vertices, edge factor 16); vHong -p 1 -q 1; 120 GB device budget; "
+                      "latency = submit to labels in host memory"),
 }
 
 
@@ -385,6 +389,117 @@ def run_batch(args):
     eng.close()
 
 
+def run_serve(args):
+    """cfg5: p50 / p99 latency and graphs/s of the request server."""
+    import threading
+
+    import torch
+
+    import detectingscc_b200 as scc
+    from detectingscc_b200 import graphs
+    world, rank, local = _dist_init()
+    torch.cuda.set_device(local)
+    cfg = CONFIGS["cfg5"]
+    rate = 2000.0
+    duration = float(args.scale or max(args.steps, 30))
+    rng = np.random.default_rng(7 + rank)
+
+    def pinned_graph(g):
+        arrs = []
+        for a in (g.Fr, g.Fc, g.Br, g.Bc):
+            t = torch.from_numpy(a.view(np.int32)).pin_memory()
+            arrs.append(t)
+        h = scc.Graph(g.V, g.E, *(t.numpy().view(np.uint32) for t in arrs))
+        h._pins = arrs
+        return h
+
+    small = [pinned_graph(g) for g in _batch_graphs(512, seed=11 + rank)]
+    large = []
+    for k in range(4):
+        V, s_, d_ = graphs.rmat(20, seed=100 + k + 10 * rank, device=torch.device("cuda", local))
+        large.append(pinned_graph(graphs.to_graph(V, s_, d_)))
+    # solo answers for the in-mix check
+    eng = scc.Engine(local)
+    solo = {}
+    for i, g in enumerate(small + large):
+        r = eng.run(g, algo=cfg["algo"], t1=cfg["t1"], t2=cfg["t2"])
+        solo[i] = r.labels.copy()
+    eng.close()
+    srv = scc.Server(local, algo=cfg["algo"], t1=cfg["t1"], t2=cfg["t2"], budget_bytes=120 * 10**9)
+    # warm-up: every large graph and a burst of small ones
+    for g in large + small[:64]:
+        srv.submit(g)
+    got = 0
+    while got < len(large) + 64:
+        got += len(srv.poll(256, wait_ms=100))
+    lat, qms, done, checked, bad, edges = [], [], 0, 0, 0, 0
+    pool_of = {}
+    stop = threading.Event()
+    sent = [0]
+
+    def producer():
+        t_next = time.perf_counter()
+        t_end = t_next + duration
+        while True:
+            t_next += rng.exponential(1.0 / rate)
+            if t_next > t_end:
+                break
+            d = t_next - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            if rng.random() < 0.05:
+                i = len(small) + int(rng.integers(len(large)))
+                g = large[i - len(small)]
+            else:
+                i = int(rng.integers(len(small)))
+                g = small[i]
+            pool_of[srv.submit(g)] = i
+            sent[0] += 1
+        stop.set()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    th = threading.Thread(target=producer, daemon=True)
+    t0 = time.perf_counter()
+    th.start()
+    while not (stop.is_set() and done >= sent[0]):
+        for r in srv.poll(1024, wait_ms=50):
+            i = pool_of.pop(r["ticket"], None)
+            done += 1
+            if r["status"] != 0:
+                bad += 1
+                continue
+            lat.append(r["latency_ms"])
+            qms.append(r["queue_ms"])
+            g = small[i] if i < len(small) else large[i - len(small)]
+            edges += g.E
+            if done % 17 == 0 or i >= len(small):   # bit-exact check against the solo run
+                checked += 1
+                bad += int(not np.array_equal(r["labels"], solo[i]))
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    info = srv.info()
+    srv.close()
+    lat = np.array(lat)
+    out = {
+        "metric": "serving SCC p99 latency (cfg5)", "value": round(float(np.percentile(lat, 99)), 3), "unit": "ms",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded generator, no dataset)",
+        "config": {"workload": f"cfg5: {cfg['desc']}", "duration_s": duration, "rate_req_per_s": rate,
+                   "pool": {"small_graphs": len(small), "large_graphs": len(large)},
+                   "parallelism": "one server per rank" if world > 1 else "single GPU"},
+        "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
+        "p50_queue_ms": round(float(np.percentile(qms, 50)), 3),
+        "graphs_per_s": round(done / wall, 1), "Medges_per_s": round(edges / wall / 1e6, 1),
+        "requests": int(done), "failed_or_mismatched": int(bad), "checked_bit_exact": int(checked),
+        "server": info, "e2e": {"value": round(done / wall, 1), "unit": "graphs/s",
+                                "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
+        "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
 def run_reference(args):
     world, rank, local = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), \
         int(os.environ.get("LOCAL_RANK", "0"))
@@ -498,6 +613,8 @@ def main():
         run_reference(args)
     elif args.config == "cfg4":
         run_batch(args)
+    elif args.config == "cfg5":
+        run_serve(args)
     else:
         run_ours(args)
 
