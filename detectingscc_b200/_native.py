@@ -85,7 +85,7 @@ C_SYMBOLS = ["scc_create", "scc_destroy", "scc_run", "scc_set_tuning", "scc_stat
              "scc_batch_autotune", "scc_batch_info", "scc_server_create", "scc_server_submit",
              "scc_server_poll", "scc_server_info", "scc_server_destroy"]
 CXX_SYMBOLS = ["_Z5vHongjjPjS_S_S_bb", "_Z6vSlotajjPjS_S_S_bb", "_Z5wHongjjPjS_S_S_bbi",
-               "_Z6wSlotajjPjS_S_S_bbi", "_Z13loadFullGraphPKcPjS1_PS1_S2_S2_S2_S2_"]
+               "_Z6wSlotajjPjS_S_S_bbi", "_Z13loadFullGraphPKcPjS1_PS1_S2_S2_S2_S2_", "_Z9detectSCCjjPjS_S_S_S_bb"]
 
 _lib = None
 

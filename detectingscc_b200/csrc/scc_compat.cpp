@@ -88,3 +88,13 @@ void wSlota(uint32_t CSize, uint32_t RSize, uint32_t *Fc, uint32_t *Fr, uint32_t
 {
     run_or_die(SCC_ALGO_WSLOTA, CSize, RSize, Fc, Fr, Bc, Br, t1, t2, warpSize);
 }
+
+// detectSCC (scc.h:53, scc_WCC.cu:1000-1617) -- the METIS-partitioned
+// experiment -- is not provided.  The symbol exists so that the reference's
+// own scc.cu links unchanged; calling it throws a const char*, which the
+// reference's main catches, prints and turns into exit status 1
+// (scc.cu:104-108).
+void detectSCC(uint32_t, uint32_t, uint32_t *, uint32_t *, uint32_t *, uint32_t *, uint32_t *, bool, bool)
+{
+    throw "detectSCC (-a d) is not provided by this engine";
+}
