@@ -297,6 +297,17 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def _pinned_graph(g):
+    """The graph's CSR arrays copied into page-locked host memory."""
+    import torch
+
+    import detectingscc_b200 as scc
+    arrs = [torch.from_numpy(a.view(np.int32)).pin_memory() for a in (g.Fr, g.Fc, g.Br, g.Bc)]
+    h = scc.Graph(g.V, g.E, *(t.numpy().view(np.uint32) for t in arrs))
+    h._pins = arrs
+    return h
+
+
 def _batch_graphs(n_graphs: int, seed: int = 1):
     import concurrent.futures as cf
 
@@ -321,6 +332,7 @@ def run_batch(args):
     b = scc.Batch(eng, gs)
     t_ins = time.perf_counter()
     best_t, best_q, _ = b.autotune(algo=cfg["algo"], t1=cfg["t1"], t2=cfg["t2"], warp=cfg["warp"])
+    best_c, best_big, n_cl = b.cluster()
     t_tune = time.perf_counter() - t_ins
     for _ in range(args.warmup):
         b.run(algo=cfg["algo"], t1=cfg["t1"], t2=cfg["t2"], warp=cfg["warp"], labels=False)
@@ -342,13 +354,16 @@ def run_batch(args):
         seq.append(st_s["kernel_ms"])
     t_seq = _max_over_ranks(sum(seq) / len(seq), world)
     assert [r[0] for r in res] == [r[0] for r in res_s]
-    # end to end: upload every graph from host memory, run, read all labels back
+    # end to end: upload every graph from (page-locked) host memory, run, read all labels back
+    import torch as _t
+    pins = [_pinned_graph(g) for g in gs]
+    hlab = _t.zeros(b.total_vertices, dtype=_t.int32).pin_memory().numpy().view(np.uint32)
     e2e = []
-    hlab = np.zeros(b.total_vertices, dtype=np.uint32)
     for _ in range(max(1, min(3, args.steps))):
         t0 = time.perf_counter()
-        b2 = scc.Batch(eng, gs)
+        b2 = scc.Batch(eng, pins)
         b2.set_schedule(best_t, best_q)
+        b2.set_cluster(best_c, best_big)
         b2.run(algo=cfg["algo"], t1=cfg["t1"], t2=cfg["t2"], warp=cfg["warp"], out=hlab)
         e2e.append(time.perf_counter() - t0)
         b2.close()
@@ -360,7 +375,8 @@ def run_batch(args):
         "ms_per_step": round(t_batch, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u32", "data": "synthetic (seeded generator, no dataset)",
         "config": {"workload": f"cfg4: {cfg['desc']}", "graphs": n_graphs, "sum_V": b.total_vertices,
-                   "sum_E": sumE, "seed": 1, "schedule": {"threads": best_t, "qcap": best_q,
+                   "sum_E": sumE, "seed": 1, "schedule": {"threads": best_t, "qcap": best_q, "cluster": best_c,
+                                                          "big_vertices": best_big, "cluster_graphs": n_cl,
                                                           "autotune_s": round(t_tune, 2)},
                    "l2": "inputs larger than L2", "parallelism": "graphs sharded per rank" if world > 1 else "single GPU"},
         "per_graph_plain": {"ms_per_batch": round(t_seq, 3), "graphs_per_s": round(world * n_graphs / (t_seq * 1e-3), 1)},
@@ -404,35 +420,25 @@ def run_serve(args):
     duration = float(args.scale or max(args.steps, 30))
     rng = np.random.default_rng(7 + rank)
 
-    def pinned_graph(g):
-        arrs = []
-        for a in (g.Fr, g.Fc, g.Br, g.Bc):
-            t = torch.from_numpy(a.view(np.int32)).pin_memory()
-            arrs.append(t)
-        h = scc.Graph(g.V, g.E, *(t.numpy().view(np.uint32) for t in arrs))
-        h._pins = arrs
-        return h
-
-    small = [pinned_graph(g) for g in _batch_graphs(512, seed=11 + rank)]
+    small = [_pinned_graph(g) for g in _batch_graphs(512, seed=11 + rank)]
     large = []
     for k in range(4):
         V, s_, d_ = graphs.rmat(20, seed=100 + k + 10 * rank, device=torch.device("cuda", local))
-        large.append(pinned_graph(graphs.to_graph(V, s_, d_)))
+        large.append(_pinned_graph(graphs.to_graph(V, s_, d_)))
+    pool = small + large
     # solo answers for the in-mix check
     eng = scc.Engine(local)
-    solo = {}
-    for i, g in enumerate(small + large):
-        r = eng.run(g, algo=cfg["algo"], t1=cfg["t1"], t2=cfg["t2"])
-        solo[i] = r.labels.copy()
+    solo = [eng.run(g, algo=cfg["algo"], t1=cfg["t1"], t2=cfg["t2"]).labels.copy() for g in pool]
     eng.close()
     srv = scc.Server(local, algo=cfg["algo"], t1=cfg["t1"], t2=cfg["t2"], budget_bytes=120 * 10**9)
     # warm-up: every large graph and a burst of small ones
-    for g in large + small[:64]:
-        srv.submit(g)
-    got = 0
-    while got < len(large) + 64:
-        got += len(srv.poll(256, wait_ms=100))
-    lat, qms, done, checked, bad, edges = [], [], 0, 0, 0, 0
+    for _ in range(max(args.warmup, 1)):
+        for g in large + small[:64]:
+            srv.submit(g)
+        got = 0
+        while got < len(large) + 64:
+            got += len(srv.poll(256, wait_ms=100))
+    lat_s, lat_l, qms, done, checked, bad, edges, h2d, d2h = [], [], [], 0, 0, 0, 0, 0, 0
     pool_of = {}
     stop = threading.Event()
     sent = [0]
@@ -447,54 +453,59 @@ def run_serve(args):
             d = t_next - time.perf_counter()
             if d > 0:
                 time.sleep(d)
-            if rng.random() < 0.05:
-                i = len(small) + int(rng.integers(len(large)))
-                g = large[i - len(small)]
-            else:
-                i = int(rng.integers(len(small)))
-                g = small[i]
-            pool_of[srv.submit(g)] = i
+            i = len(small) + int(rng.integers(len(large))) if rng.random() < 0.05 else int(rng.integers(len(small)))
+            pool_of[srv.submit(pool[i])] = i
             sent[0] += 1
         stop.set()
 
+    launches0 = srv.launches()
     clocks = ClockSampler(local)
     clocks.start()
     th = threading.Thread(target=producer, daemon=True)
     t0 = time.perf_counter()
     th.start()
     while not (stop.is_set() and done >= sent[0]):
-        for r in srv.poll(1024, wait_ms=50):
+        for r in srv.poll(1024, wait_ms=20):
             i = pool_of.pop(r["ticket"], None)
             done += 1
             if r["status"] != 0:
                 bad += 1
                 continue
-            lat.append(r["latency_ms"])
+            (lat_l if i >= len(small) else lat_s).append(r["latency_ms"])
             qms.append(r["queue_ms"])
-            g = small[i] if i < len(small) else large[i - len(small)]
+            g = pool[i]
             edges += g.E
+            h2d += g.nbytes
+            d2h += 4 * g.V
             if done % 17 == 0 or i >= len(small):   # bit-exact check against the solo run
                 checked += 1
                 bad += int(not np.array_equal(r["labels"], solo[i]))
     wall = time.perf_counter() - t0
     clk = clocks.stop()
     info = srv.info()
+    launches = srv.launches() - launches0
     srv.close()
-    lat = np.array(lat)
+    lat = np.array(lat_s + lat_l)
+    pct = lambda a, q: round(float(np.percentile(a, q)), 3) if len(a) else None  # noqa: E731
     out = {
-        "metric": "serving SCC p99 latency (cfg5)", "value": round(float(np.percentile(lat, 99)), 3), "unit": "ms",
+        "metric": "serving SCC p99 latency (cfg5)", "value": pct(lat, 99), "unit": "ms",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded generator, no dataset)",
         "config": {"workload": f"cfg5: {cfg['desc']}", "duration_s": duration, "rate_req_per_s": rate,
                    "pool": {"small_graphs": len(small), "large_graphs": len(large)},
+                   "server": {"lanes": 8, "batch_threads": 1024, "qcap": 256, "cluster": 4, "big_vertices": 16384,
+                              "large_cluster": 16},
+                   "inputs": "page-locked host CSR per request, labels to pageable host arrays",
                    "parallelism": "one server per rank" if world > 1 else "single GPU"},
-        "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
-        "p50_queue_ms": round(float(np.percentile(qms, 50)), 3),
+        "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99), "p50_queue_ms": pct(qms, 50),
+        "small": {"p50_ms": pct(lat_s, 50), "p99_ms": pct(lat_s, 99), "n": len(lat_s)},
+        "large": {"p50_ms": pct(lat_l, 50), "p99_ms": pct(lat_l, 99), "n": len(lat_l)},
         "graphs_per_s": round(done / wall, 1), "Medges_per_s": round(edges / wall / 1e6, 1),
         "requests": int(done), "failed_or_mismatched": int(bad), "checked_bit_exact": int(checked),
-        "server": info, "e2e": {"value": round(done / wall, 1), "unit": "graphs/s",
-                                "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
-        "clocks": clk,
+        "server_info": info,
+        "e2e": {"value": round(done / wall, 1), "unit": "graphs/s", "step": "one request",
+                "h2d_bytes_per_step": int(h2d / max(done, 1)), "d2h_bytes_per_step": int(d2h / max(done, 1))},
+        "gpu_launches": int(launches), "clocks": clk,
     }
     if rank == 0:
         print(json.dumps(out), flush=True)

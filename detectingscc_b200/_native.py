@@ -48,7 +48,7 @@ class HostGraph(ctypes.Structure):
 class ServerConfig(ctypes.Structure):
     _fields_ = [("budget_bytes", u64), ("lanes", u32), ("max_graphs_per_batch", u32), ("large_vertices", u32),
                 ("batch_threads", ctypes.c_int32), ("qcap", u32), ("algo", ctypes.c_int32), ("flags", u32),
-                ("warp_width", ctypes.c_int32)]
+                ("warp_width", ctypes.c_int32), ("cluster", u32), ("big_vertices", u32), ("large_cluster", u32)]
 
 
 class ServerResult(ctypes.Structure):
@@ -82,8 +82,8 @@ C_SYMBOLS = ["scc_create", "scc_destroy", "scc_run", "scc_set_tuning", "scc_stat
              "scc_version", "scc_get_trace", "scc_load_graph", "scc_save_binary", "scc_graph_from_arcs",
              "scc_free_host_graph", "scc_reference_call", "scc_batch_create", "scc_batch_run",
              "scc_batch_destroy", "scc_run_noalloc", "scc_batch_set_schedule", "scc_batch_get_schedule",
-             "scc_batch_autotune", "scc_batch_info", "scc_server_create", "scc_server_submit",
-             "scc_server_poll", "scc_server_info", "scc_server_destroy"]
+             "scc_batch_autotune", "scc_batch_info", "scc_batch_set_cluster", "scc_batch_get_cluster", "scc_server_create", "scc_server_submit",
+             "scc_server_poll", "scc_server_info", "scc_server_launches", "scc_server_destroy"]
 CXX_SYMBOLS = ["_Z5vHongjjPjS_S_S_bb", "_Z6vSlotajjPjS_S_S_bb", "_Z5wHongjjPjS_S_S_bbi",
                "_Z6wSlotajjPjS_S_S_bbi", "_Z13loadFullGraphPKcPjS1_PS1_S2_S2_S2_S2_", "_Z9detectSCCjjPjS_S_S_S_bb"]
 
@@ -135,12 +135,15 @@ def lib():
     L.scc_batch_autotune.argtypes = [vp, ctypes.c_int, u32, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                      ctypes.POINTER(u32), ctypes.POINTER(ctypes.c_float)]
     L.scc_batch_info.argtypes = [vp, ctypes.POINTER(u64), ctypes.POINTER(u64), ctypes.POINTER(u32)]
+    L.scc_batch_set_cluster.argtypes = [vp, ctypes.c_int, u32]
+    L.scc_batch_get_cluster.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(u32), ctypes.POINTER(u32)]
     L.scc_run_noalloc.argtypes = [ctypes.POINTER(CsrView), ctypes.c_int, u32, ctypes.c_int, vp,
                                   ctypes.POINTER(Stats), vp]
     L.scc_server_create.argtypes = [ctypes.c_int, ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]
     L.scc_server_submit.argtypes = [vp, ctypes.POINTER(CsrView), vp, ctypes.POINTER(u64)]
     L.scc_server_poll.argtypes = [vp, ctypes.POINTER(ServerResult), u32, ctypes.POINTER(u32), ctypes.c_int]
     L.scc_server_info.argtypes = [vp, ctypes.POINTER(u64), ctypes.POINTER(u64), ctypes.POINTER(u64), ctypes.POINTER(u64)]
+    L.scc_server_launches.argtypes = [vp, ctypes.POINTER(u64)]
     L.scc_server_destroy.argtypes = [vp]
     L.scc_get_trace.argtypes = [vp, ctypes.POINTER(u64), u32, ctypes.POINTER(u32), ctypes.POINTER(u64)]
     _lib = L

@@ -207,6 +207,16 @@ class Batch:
         N.check(self._lib.scc_batch_get_schedule(self._h, ctypes.byref(t), ctypes.byref(q)))
         return t.value, q.value
 
+    def set_cluster(self, cluster: int, big_vertices: int = 16384) -> None:
+        """Run graphs with at least big_vertices vertices on clusters of `cluster` CTAs (1: off)."""
+        N.check(self._lib.scc_batch_set_cluster(self._h, int(cluster), int(big_vertices)), "scc_batch_set_cluster")
+
+    def cluster(self):
+        """(cluster size, big_vertices, number of graphs that run on whole clusters)."""
+        c, b, n = ctypes.c_int(0), ctypes.c_uint32(0), ctypes.c_uint32(0)
+        N.check(self._lib.scc_batch_get_cluster(self._h, ctypes.byref(c), ctypes.byref(b), ctypes.byref(n)))
+        return c.value, b.value, n.value
+
     def autotune(self, algo="h", t1=True, t2=True, warp=1):
         t, q, ms = ctypes.c_int(0), ctypes.c_uint32(0), ctypes.c_float(0)
         flags = (N.FLAG_TRIM1 if t1 else 0) | (N.FLAG_TRIM2 if t2 else 0)
@@ -241,11 +251,13 @@ class Server:
     """
 
     def __init__(self, device: int = 0, algo="h", t1=True, t2=True, warp=1, budget_bytes: int = 0, lanes: int = 0,
-                 max_graphs_per_batch: int = 0, large_vertices: int = 0, batch_threads: int = 0, qcap: int = 0):
+                 max_graphs_per_batch: int = 0, large_vertices: int = 0, batch_threads: int = 0, qcap: int = 0,
+                 cluster: int = 0, big_vertices: int = 0, large_cluster: int = 0):
         self._lib = N.lib()
         cfg = N.ServerConfig(int(budget_bytes), int(lanes), int(max_graphs_per_batch), int(large_vertices),
                              int(batch_threads), int(qcap), _algo_code(algo),
-                             (N.FLAG_TRIM1 if t1 else 0) | (N.FLAG_TRIM2 if t2 else 0), int(warp))
+                             (N.FLAG_TRIM1 if t1 else 0) | (N.FLAG_TRIM2 if t2 else 0), int(warp),
+                             int(cluster), int(big_vertices), int(large_cluster))
         h = ctypes.c_void_p()
         N.check(self._lib.scc_server_create(int(device), ctypes.byref(cfg), ctypes.byref(h)), "scc_server_create")
         self._h = h
@@ -277,6 +289,12 @@ class Server:
         a, b, c, d = (ctypes.c_uint64(0) for _ in range(4))
         N.check(self._lib.scc_server_info(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(d)))
         return {"pending": a.value, "completed": b.value, "held_bytes": c.value, "rejected": d.value}
+
+    def launches(self) -> int:
+        """Kernel launches made so far."""
+        n = ctypes.c_uint64(0)
+        N.check(self._lib.scc_server_launches(self._h, ctypes.byref(n)))
+        return n.value
 
     def close(self):
         if getattr(self, "_h", None):

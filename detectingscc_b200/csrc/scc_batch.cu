@@ -13,8 +13,10 @@
 // (scc_run on device pointers into the arena, one after the other on one
 // stream): the baseline the batched launch is measured against.
 //
-// Schedules (CTA size 128 / 256 / 512 / 1024 threads, staging slice size)
-// are picked by scc_batch_autotune, which times candidates on the batch.
+// Schedules (CTA size 128 / 256 / 512 / 1024 threads, staging slice size,
+// cluster size and the vertex count from which a graph runs on a whole
+// cluster) are picked by scc_batch_autotune, which times candidates on the
+// batch.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -27,64 +29,100 @@
 #include "scc_internal.h"
 #include "scc_phases.cuh"
 
+#include <cooperative_groups.h>
+
 using namespace sccb;
 
 #include "scc_batch_internal.h"
 
 namespace {
 
+// Runs one graph with execution policy `ex` on the scratch slice `base`
+// (every CTA of the policy calls it with the same arguments).
+template <bool HONG, class Ex>
+__device__ void batch_one(Ex &ex, const BatchParams &p, uint32_t gi, char *base, Work &s_w)
+{
+    const BatchGraph bg = p.graphs[gi];
+    if (bg.V == 0u) {
+        if (ex.leader()) {
+            p.res[gi] = BatchRes{0ull, 0ull, 0ull, 0, 0};
+            if (p.done) {
+                __threadfence_system();
+                *(volatile unsigned *)&p.done[gi] = 1u;
+            }
+        }
+        return;
+    }
+    Graph g{bg.V, bg.E, p.Fr + bg.off_r, p.Fc + bg.off_c, p.Br + bg.off_r, p.Bc + bg.off_c, p.vec};
+    if (threadIdx.x == 0) {
+        carve_work(base, bg.V, bg.E, HONG, &s_w);
+        s_w.qcap = p.qcap;
+        s_w.bu_k = p.bu_k;
+    }
+    __syncthreads();
+    const Work &w = s_w;
+    ex.ctl = w.ctl;
+    // fresh control block and pivot table for this graph
+    {
+        uint32_t *c = reinterpret_cast<uint32_t *>(w.ctl);
+        for (unsigned i = ex.tid(); i < sizeof(Ctl) / 4; i += ex.nthr()) c[i] = 0u;
+        const uint32_t npk = HONG ? 4u * (bg.V + 1u) + 8u : 1u;
+        for (uint32_t i = ex.tid(); i < npk; i += ex.nthr()) w.pivkey[i] = 0ull;
+        ex.sync();
+        if (ex.leader()) w.ctl->timeout_ns = p.timeout_ns;
+        ex.sync();
+    }
+    ex.gl = 0u;
+    Carry cy{0u, 0u, 0u};
+    int rc = HONG ? hong_front(ex, g, w, p.t1, p.t2, p.lw, cy) : slota_front(ex, g, w, p.t1, p.lw, cy);
+    if (rc == RUN_DONE) rc = HONG ? hong_loop(ex, g, w, cy, 0u) : slota_peels(ex, g, w, cy, 0u);
+    ex.sync();   // the same error word in every CTA of the policy
+    const int err = *(volatile int *)&w.ctl->error;
+    if (!err) {
+        uint32_t *o = p.out + bg.off_out;
+        for (uint32_t v = ex.tid() + 1u; v <= bg.V; v += ex.nthr()) {
+            const uint32_t l = w.label[v];
+            o[v - 1u] = l <= bg.V ? w.smin[l] : 0u;
+        }
+    }
+    if (ex.leader()) p.res[gi] = BatchRes{w.ctl->n_trim1, w.ctl->n_trim2, w.ctl->n_pivot, err, w.ctl->where};
+    if (p.done) __threadfence_system();   // labels and result reach the host before the flag
+    ex.sync();   // the slice is reused by the next graph
+    if (p.done && ex.leader()) *(volatile unsigned *)&p.done[gi] = 1u;
+}
+
+// The first p.nbig graphs of p.order run one at a time on a whole cluster
+// (when the launch has clusters), the rest one per CTA.  Counters:
+// next[0] for cluster graphs, next[1] for CTA graphs.
 template <int THREADS, bool HONG>
 __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_scc_batch(BatchParams p)
 {
-    __shared__ uint32_t s_k;
+    __shared__ uint32_t s_k, s_kb;
     __shared__ Work s_w;   // per-graph carving, kept in shared memory rather than local memory
     bq_init();
     char *mine = p.scratch + (size_t)blockIdx.x * p.scratch_per_cta;
+    if (p.nbig) {
+        const unsigned cr = cluster_rank(), cn = cluster_size();
+        char *lead = p.scratch + (size_t)((blockIdx.x - cr) / p.lead_div) * p.scratch_per_cta;   // 1-D clusters
+        for (;;) {
+            if (cr == 0 && threadIdx.x == 0) s_kb = atomicAdd(&p.next[0], 1u);
+            cluster_barrier();
+            const uint32_t k = *cooperative_groups::this_cluster().map_shared_rank(&s_kb, 0);
+            cluster_barrier();   // rank 0 rewrites s_kb only after every CTA has read it
+            if (k >= p.nbig) break;
+            ClusterExec<false> ex{nullptr, 0u, cr, cn, p.cbar ? p.cbar + (blockIdx.x - cr) / cn : nullptr,
+                                  p.timeout_ns};
+            batch_one<HONG>(ex, p, p.order[k], lead, s_w);
+        }
+    }
     for (;;) {
         __syncthreads();
-        if (threadIdx.x == 0) s_k = atomicAdd(p.next, 1u);
+        if (threadIdx.x == 0) s_k = p.nbig + atomicAdd(&p.next[1], 1u);
         __syncthreads();
         const uint32_t k = s_k;
         if (k >= p.n) return;
-        const uint32_t gi = p.order[k];
-        const BatchGraph bg = p.graphs[gi];
-        if (bg.V == 0u) {
-            if (threadIdx.x == 0) p.res[gi] = BatchRes{0ull, 0ull, 0ull, 0, 0};
-            continue;
-        }
-        Graph g{bg.V, bg.E, p.Fr + bg.off_r, p.Fc + bg.off_c, p.Br + bg.off_r, p.Bc + bg.off_c, p.vec};
-        if (threadIdx.x == 0) {
-            carve_work(mine, bg.V, bg.E, HONG, &s_w);
-            s_w.qcap = p.qcap;
-            s_w.bu_k = p.bu_k;
-        }
-        __syncthreads();
-        const Work &w = s_w;
-        // fresh control block and pivot table for this graph
-        {
-            uint32_t *c = reinterpret_cast<uint32_t *>(w.ctl);
-            for (unsigned i = threadIdx.x; i < sizeof(Ctl) / 4; i += blockDim.x) c[i] = 0u;
-            const uint32_t npk = HONG ? 4u * (bg.V + 1u) + 8u : 1u;
-            for (uint32_t i = threadIdx.x; i < npk; i += blockDim.x) w.pivkey[i] = 0ull;
-            __syncthreads();
-            if (threadIdx.x == 0) w.ctl->timeout_ns = p.timeout_ns;
-            __syncthreads();
-        }
-        BlockExec<false> ex{w.ctl, 0u};
-        Carry cy{0u, 0u, 0u};
-        int rc = HONG ? hong_front(ex, g, w, p.t1, p.t2, p.lw, cy) : slota_front(ex, g, w, p.t1, p.lw, cy);
-        if (rc == RUN_DONE) rc = HONG ? hong_loop(ex, g, w, cy, 0u) : slota_peels(ex, g, w, cy, 0u);
-        __syncthreads();
-        const int err = *(volatile int *)&w.ctl->error;
-        if (!err) {
-            uint32_t *o = p.out + bg.off_out;
-            for (uint32_t v = threadIdx.x + 1u; v <= bg.V; v += blockDim.x) {
-                const uint32_t l = w.label[v];
-                o[v - 1u] = l <= bg.V ? w.smin[l] : 0u;
-            }
-        }
-        if (threadIdx.x == 0)
-            p.res[gi] = BatchRes{w.ctl->n_trim1, w.ctl->n_trim2, w.ctl->n_pivot, err, w.ctl->where};
+        BlockExec<false> ex{nullptr, 0u};
+        batch_one<HONG>(ex, p, p.order[k], mine, s_w);
     }
 }
 
@@ -110,36 +148,104 @@ size_t batch_smem(int threads, uint32_t qcap) { return (BQ_HDR + NBQ * (size_t)(
 
 size_t sccb_batch_smem(int threads, uint32_t qcap) { return batch_smem(threads, qcap); }
 
-int sccb_batch_ctas(int threads, uint32_t qcap, int nsm, uint32_t *out)
+int sccb_batch_ctas(int threads, uint32_t qcap, int nsm, uint32_t *out, int cluster)
 {
     const size_t smem = batch_smem(threads, qcap);
-    for (int h = 0; h < 2; h++)
-        if (cudaFuncSetAttribute(pick_batch_kernel(threads, h != 0), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem) != cudaSuccess) {
+    for (int h = 0; h < 2; h++) {
+        void *fn = pick_batch_kernel(threads, h != 0);
+        if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+            (cluster > 8 && cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)) {
             cudaGetLastError();
             return SCC_ERR_CUDA;
         }
-    int occ = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pick_batch_kernel(threads, true), threads, smem) !=
-            cudaSuccess || occ <= 0) {
+    }
+    if (cluster <= 1) {
+        int occ = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pick_batch_kernel(threads, true), threads, smem) !=
+                cudaSuccess || occ <= 0) {
+            cudaGetLastError();
+            return SCC_ERR_CUDA;
+        }
+        *out = (uint32_t)(occ * nsm);
+        return SCC_OK;
+    }
+    // clusters resident at once (a cluster sits inside one GPC)
+    cudaLaunchConfig_t cfg{};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3((unsigned)cluster * (unsigned)nsm);
+    cfg.blockDim = dim3((unsigned)threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int ncl = 0;
+    if (cudaOccupancyMaxActiveClusters(&ncl, pick_batch_kernel(threads, true), &cfg) != cudaSuccess || ncl <= 0) {
         cudaGetLastError();
         return SCC_ERR_CUDA;
     }
-    *out = (uint32_t)(occ * nsm);
+    *out = (uint32_t)(ncl * cluster);
     return SCC_OK;
 }
 
-int sccb_batch_launch(const BatchParams &p, int threads, bool hong, uint32_t ncta, cudaStream_t st)
+int sccb_batch_launch(const BatchParams &p, int threads, bool hong, uint32_t ncta, cudaStream_t st, int cluster)
 {
     BatchParams q = p;
     void *args[] = {&q};
-    cudaError_t e = cudaLaunchKernel(pick_batch_kernel(threads, hong), dim3(ncta), dim3(threads), args,
-                                     batch_smem(threads, p.qcap), st);
+    cudaError_t e;
+    if (cluster <= 1) {
+        e = cudaLaunchKernel(pick_batch_kernel(threads, hong), dim3(ncta), dim3(threads), args,
+                             batch_smem(threads, p.qcap), st);
+    } else {
+        cudaLaunchConfig_t cfg{};
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = (unsigned)cluster;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(ncta);
+        cfg.blockDim = dim3((unsigned)threads);
+        cfg.dynamicSmemBytes = batch_smem(threads, p.qcap);
+        cfg.stream = st;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        e = cudaLaunchKernelExC(&cfg, pick_batch_kernel(threads, hong), args);
+    }
     if (e != cudaSuccess) {
         cudaGetLastError();
         return SCC_ERR_CUDA;
     }
     return SCC_OK;
+}
+
+// CTAs of a launch over n graphs: at most the resident CTAs, a whole number
+// of clusters.
+uint32_t sccb_launch_ctas(uint32_t resident, uint32_t n, uint32_t nbig, int cluster)
+{
+    const uint32_t cs = cluster > 1 ? (uint32_t)cluster : 1u;
+    const unsigned long long want = (unsigned long long)nbig * cs + (n - nbig);
+    unsigned long long c = std::min<unsigned long long>(resident, std::max<unsigned long long>(want, 1ull));
+    c = (c + cs - 1) / cs * cs;
+    if (c > resident) c = resident / cs * cs;
+    return (uint32_t)std::max<unsigned long long>(c, cs);
+}
+
+// Processing order: graphs with at least big_vertices vertices first (they
+// run on whole clusters), then the rest, each part largest first.
+uint32_t sccb_order(const BatchGraph *g, uint32_t n, uint32_t big_vertices, int cluster, uint32_t *order)
+{
+    const bool use = cluster > 1;
+    std::iota(order, order + n, 0u);
+    auto big = [&](uint32_t i) { return use && g[i].V >= big_vertices; };
+    std::stable_sort(order, order + n, [&](uint32_t a, uint32_t c) {
+        if (big(a) != big(c)) return big(a);
+        return (unsigned long long)g[a].E + g[a].V > (unsigned long long)g[c].E + g[c].V;
+    });
+    uint32_t nb = 0;
+    while (nb < n && big(order[nb])) nb++;
+    return nb;
 }
 
 struct scc_batch {
@@ -152,6 +258,7 @@ struct scc_batch {
     std::vector<BatchGraph> hgraphs;
     BatchRes *dres = nullptr, *hres = nullptr;
     unsigned *dnext = nullptr;
+    unsigned *dcbar = nullptr;       // per-cluster software barrier words (check mode)
     char *scratch = nullptr;
     size_t scratch_bytes = 0, scratch_per_cta = 0;
     uint32_t ncta = 0;
@@ -159,10 +266,13 @@ struct scc_batch {
     cudaEvent_t ev[2] = {nullptr, nullptr};
     int threads = 256;
     uint32_t qcap = 256;
+    int cluster = 1;                 // CTAs per cluster (1: every graph on one CTA)
+    uint32_t big_vertices = 16384;   // graphs with at least this many vertices run on a whole cluster
+    uint32_t nbig = 0;
     // captured launch
     cudaGraphExec_t gexec = nullptr;
-    int g_algo = 0, g_w = 0, g_threads = 0;
-    uint32_t g_flags = 0, g_qcap = 0;
+    int g_algo = 0, g_w = 0, g_threads = 0, g_cluster = 0, g_check = 0;
+    uint32_t g_flags = 0, g_qcap = 0, g_big = 0;
 };
 
 static void batch_free(scc_batch *b)
@@ -170,30 +280,34 @@ static void batch_free(scc_batch *b)
     if (!b) return;
     if (b->gexec) cudaGraphExecDestroy(b->gexec);
     cudaFree(b->dFr); cudaFree(b->dFc); cudaFree(b->dBr); cudaFree(b->dBc); cudaFree(b->dout);
-    cudaFree(b->dorder); cudaFree(b->dgraphs); cudaFree(b->dres); cudaFree(b->dnext); cudaFree(b->scratch);
+    cudaFree(b->dorder); cudaFree(b->dgraphs); cudaFree(b->dres); cudaFree(b->dnext); cudaFree(b->dcbar); cudaFree(b->scratch);
     if (b->hres) cudaFreeHost(b->hres);
     for (auto &e : b->ev) if (e) cudaEventDestroy(e);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
 }
 
-// Scratch for the resident CTAs of the current schedule (grown on demand).
-static int batch_reserve_scratch(scc_batch *b, int threads, uint32_t qcap)
+// Processing order and cluster-graph count for the current cluster schedule.
+static int batch_upload_order(scc_batch *b, int cluster, uint32_t big_vertices)
 {
-    void *fn = pick_batch_kernel(threads, true);
-    const size_t smem = batch_smem(threads, qcap);
-    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
-        cudaFuncSetAttribute(pick_batch_kernel(threads, false), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) != cudaSuccess) {
+    std::vector<uint32_t> order(std::max<uint32_t>(b->n, 1u));
+    const uint32_t nb = sccb_order(b->hgraphs.data(), b->n, big_vertices, cluster, order.data());
+    if (b->n && (cudaMemcpyAsync(b->dorder, order.data(), (size_t)b->n * 4, cudaMemcpyHostToDevice, b->stream) != cudaSuccess ||
+                 cudaStreamSynchronize(b->stream) != cudaSuccess)) {
         cudaGetLastError();
         return SCC_ERR_CUDA;
     }
-    int occ = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, threads, smem) != cudaSuccess || occ <= 0) {
-        cudaGetLastError();
-        return SCC_ERR_CUDA;
-    }
-    const uint32_t ncta = (uint32_t)std::min<unsigned long long>((unsigned long long)occ * b->ctx->nsm, b->n ? b->n : 1);
+    b->nbig = nb;
+    return SCC_OK;
+}
+
+// Scratch for the CTAs of a schedule (grown on demand); sets b->ncta.
+static int batch_reserve_scratch(scc_batch *b, int threads, uint32_t qcap, int cluster, uint32_t nbig)
+{
+    uint32_t resident = 0;
+    int rc = sccb_batch_ctas(threads, qcap, b->ctx->nsm, &resident, cluster);
+    if (rc != SCC_OK) return rc;
+    const uint32_t ncta = sccb_launch_ctas(resident, b->n, nbig, cluster);
     const size_t need = (size_t)ncta * b->scratch_per_cta;
     if (need > b->scratch_bytes) {
         cudaFree(b->scratch);
@@ -245,7 +359,9 @@ extern "C" int scc_batch_create(scc_context *ctx, const scc_csr_view *graphs, ui
     alloc((void **)&b->dorder, (size_t)n * 4);
     alloc((void **)&b->dgraphs, (size_t)n * sizeof(BatchGraph));
     alloc((void **)&b->dres, (size_t)n * sizeof(BatchRes));
-    alloc((void **)&b->dnext, 4);
+    alloc((void **)&b->dnext, 16);
+    alloc((void **)&b->dcbar, 4096);
+    if (rc == SCC_OK && cudaMemset(b->dcbar, 0, 4096) != cudaSuccess) rc = SCC_ERR_CUDA;
     if (rc == SCC_OK && cudaMallocHost((void **)&b->hres, std::max<size_t>((size_t)n * sizeof(BatchRes), 16)) != cudaSuccess)
         rc = SCC_ERR_OOM;
     if (rc == SCC_OK && (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
@@ -263,20 +379,16 @@ extern "C" int scc_batch_create(scc_context *ctx, const scc_csr_view *graphs, ui
              cudaMemcpyAsync(b->dBc + bg.off_c, g.Bc, (size_t)g.num_edges * 4, cudaMemcpyHostToDevice, b->stream) != cudaSuccess))
             rc = SCC_ERR_CUDA;
     }
-    // largest graphs first (longest-processing-time order)
-    std::vector<uint32_t> order(n);
-    std::iota(order.begin(), order.end(), 0u);
-    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t c) {
-        return (unsigned long long)b->hgraphs[a].E + b->hgraphs[a].V > (unsigned long long)b->hgraphs[c].E + b->hgraphs[c].V;
-    });
     if (rc == SCC_OK &&
-        (cudaMemcpyAsync(b->dorder, order.data(), (size_t)n * 4, cudaMemcpyHostToDevice, b->stream) != cudaSuccess ||
-         cudaMemcpyAsync(b->dgraphs, b->hgraphs.data(), (size_t)n * sizeof(BatchGraph), cudaMemcpyHostToDevice, b->stream) != cudaSuccess ||
+        (cudaMemcpyAsync(b->dgraphs, b->hgraphs.data(), (size_t)n * sizeof(BatchGraph), cudaMemcpyHostToDevice, b->stream) != cudaSuccess ||
          cudaStreamSynchronize(b->stream) != cudaSuccess))
         rc = SCC_ERR_CUDA;
     if (rc != SCC_OK) { cudaGetLastError(); batch_free(b); return rc; }
+    // largest graphs first (longest-processing-time order)
+    rc = batch_upload_order(b, b->cluster, b->big_vertices);
+    if (rc != SCC_OK) { batch_free(b); return rc; }
     b->scratch_per_cta = carve_work(nullptr, b->maxV, b->maxE, true, nullptr);
-    rc = batch_reserve_scratch(b, b->threads, b->qcap);
+    rc = batch_reserve_scratch(b, b->threads, b->qcap, b->cluster, b->nbig);
     if (rc != SCC_OK) { batch_free(b); return rc; }
     *out = b;
     return SCC_OK;
@@ -297,10 +409,36 @@ extern "C" int scc_batch_set_schedule(scc_batch *b, int threads, uint32_t qcap)
         return SCC_ERR_INVALID_ARG;
     if (batch_smem(threads, qcap) > 200 * 1024) return SCC_ERR_INVALID_ARG;
     cudaSetDevice(b->ctx->device);
-    int rc = batch_reserve_scratch(b, threads, qcap);
+    int rc = batch_reserve_scratch(b, threads, qcap, b->cluster, b->nbig);
     if (rc != SCC_OK) return rc;
     b->threads = threads;
     b->qcap = qcap;
+    return SCC_OK;
+}
+
+extern "C" int scc_batch_set_cluster(scc_batch *b, int cluster, uint32_t big_vertices)
+{
+    if (!b || !(cluster == 1 || cluster == 2 || cluster == 4 || cluster == 8 || cluster == 16)) return SCC_ERR_INVALID_ARG;
+    cudaSetDevice(b->ctx->device);
+    int rc = batch_upload_order(b, cluster, big_vertices);
+    if (rc == SCC_OK) rc = batch_reserve_scratch(b, b->threads, b->qcap, cluster, b->nbig);
+    if (rc != SCC_OK) {
+        // back to the previous schedule
+        batch_upload_order(b, b->cluster, b->big_vertices);
+        batch_reserve_scratch(b, b->threads, b->qcap, b->cluster, b->nbig);
+        return rc;
+    }
+    b->cluster = cluster;
+    b->big_vertices = big_vertices;
+    return SCC_OK;
+}
+
+extern "C" int scc_batch_get_cluster(scc_batch *b, int *cluster, uint32_t *big_vertices, uint32_t *num_cluster_graphs)
+{
+    if (!b) return SCC_ERR_INVALID_ARG;
+    if (cluster) *cluster = b->cluster;
+    if (big_vertices) *big_vertices = b->big_vertices;
+    if (num_cluster_graphs) *num_cluster_graphs = b->nbig;
     return SCC_OK;
 }
 
@@ -360,21 +498,21 @@ extern "C" int scc_batch_run(scc_batch *b, int algo, uint32_t flags, int warp_wi
     } else {
         const uint32_t keyflags = flags & (SCC_FLAG_TRIM1 | SCC_FLAG_TRIM2);
         if (!b->gexec || b->g_algo != algo || b->g_flags != keyflags || b->g_w != warp_width ||
-            b->g_threads != b->threads || b->g_qcap != b->qcap) {
+            b->g_threads != b->threads || b->g_qcap != b->qcap || b->g_cluster != b->cluster ||
+            b->g_big != b->big_vertices || b->g_check != b->ctx->cluster_check) {
             if (b->gexec) { cudaGraphExecDestroy(b->gexec); b->gexec = nullptr; }
             BatchParams p{b->dgraphs, b->dorder, b->n, b->dFr, b->dFc, b->dBr, b->dBc, 0u, b->dout, b->dres,
-                          b->scratch, (unsigned long long)b->scratch_per_cta, b->dnext, b->qcap, b->ctx->bu_k,
+                          b->scratch, (unsigned long long)b->scratch_per_cta, b->dnext, b->nbig,
+                          b->ctx->cluster_check && b->cluster > 1 ? b->dcbar : nullptr, 1u, nullptr, b->qcap, b->ctx->bu_k,
                           (flags & SCC_FLAG_TRIM1) ? 1 : 0, (flags & SCC_FLAG_TRIM2) ? 1 : 0, lw,
                           (unsigned long long)b->ctx->timeout_ms * 1000000ull};
-            void *fn = pick_batch_kernel(b->threads, hong);
-            void *args[] = {&p};
             cudaGraph_t graph = nullptr;
             if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
                 cudaGetLastError();
                 return SCC_ERR_CUDA;
             }
-            cudaMemsetAsync(b->dnext, 0, 4, b->stream);
-            cudaLaunchKernel(fn, dim3(b->ncta), dim3(b->threads), args, batch_smem(b->threads, b->qcap), b->stream);
+            cudaMemsetAsync(b->dnext, 0, 8, b->stream);
+            sccb_batch_launch(p, b->threads, hong, b->ncta, b->stream, b->cluster);
             if (cudaStreamEndCapture(b->stream, &graph) != cudaSuccess ||
                 cudaGraphInstantiate(&b->gexec, graph, 0) != cudaSuccess) {
                 if (graph) cudaGraphDestroy(graph);
@@ -383,7 +521,8 @@ extern "C" int scc_batch_run(scc_batch *b, int algo, uint32_t flags, int warp_wi
             }
             cudaGraphDestroy(graph);
             b->g_algo = algo; b->g_flags = keyflags; b->g_w = warp_width;
-            b->g_threads = b->threads; b->g_qcap = b->qcap;
+            b->g_threads = b->threads; b->g_qcap = b->qcap; b->g_cluster = b->cluster; b->g_big = b->big_vertices;
+            b->g_check = b->ctx->cluster_check;
         }
         if (cudaGraphLaunch(b->gexec, b->stream) != cudaSuccess) { cudaGetLastError(); return SCC_ERR_CUDA; }
         cudaEventRecord(b->ev[1], b->stream);
@@ -416,31 +555,58 @@ extern "C" int scc_batch_run(scc_batch *b, int algo, uint32_t flags, int warp_wi
 }
 
 // Picks the CTA size and staging slice by timing every candidate on the
-// batch itself (one untimed and two timed runs each).
+// batch itself (one untimed and two timed runs each), then, with that
+// schedule, the cluster size and the vertex count from which graphs run on
+// whole clusters.
 extern "C" int scc_batch_autotune(scc_batch *b, int algo, uint32_t flags, int warp_width, int *best_threads,
                                   uint32_t *best_qcap, float *best_ms)
 {
     if (!b) return SCC_ERR_INVALID_ARG;
+    const uint32_t rflags = flags & ~SCC_FLAG_BATCH_SEQUENTIAL;
+    auto time_it = [&](float *ms) -> int {
+        scc_stats st;
+        int rc = scc_batch_run(b, algo, rflags, warp_width, nullptr, nullptr, &st);
+        if (rc != SCC_OK && rc < SCC_ERR_OVERFLOW) return rc;
+        *ms = 0.f;
+        for (int rep = 0; rep < 2; rep++) {
+            scc_batch_run(b, algo, rflags, warp_width, nullptr, nullptr, &st);
+            *ms += st.kernel_ms;
+        }
+        return SCC_OK;
+    };
     const int cand_t[] = {128, 256, 512, 1024};
     const uint32_t cand_q[] = {64, 256};
     float best = 1e30f;
     int bt = b->threads;
     uint32_t bq = b->qcap;
+    int rc = scc_batch_set_cluster(b, 1, b->big_vertices);
+    if (rc != SCC_OK) return rc;
     for (int t : cand_t) {
         for (uint32_t q : cand_q) {
             if (scc_batch_set_schedule(b, t, q) != SCC_OK) continue;
-            scc_stats st;
-            int rc = scc_batch_run(b, algo, flags & ~SCC_FLAG_BATCH_SEQUENTIAL, warp_width, nullptr, nullptr, &st);
-            if (rc != SCC_OK && rc < SCC_ERR_OVERFLOW) return rc;
             float ms = 0.f;
-            for (int rep = 0; rep < 2; rep++) {
-                scc_batch_run(b, algo, flags & ~SCC_FLAG_BATCH_SEQUENTIAL, warp_width, nullptr, nullptr, &st);
-                ms += st.kernel_ms;
-            }
+            rc = time_it(&ms);
+            if (rc != SCC_OK) return rc;
             if (ms < best) { best = ms; bt = t; bq = q; }
         }
     }
-    int rc = scc_batch_set_schedule(b, bt, bq);
+    rc = scc_batch_set_schedule(b, bt, bq);
+    if (rc != SCC_OK) return rc;
+    int bc = 1;
+    uint32_t bb = b->big_vertices;
+    const int cand_c[] = {2, 4, 8};
+    const uint32_t cand_b[] = {8192, 16384, 32768};
+    for (int c : cand_c) {
+        for (uint32_t v : cand_b) {
+            if (scc_batch_set_cluster(b, c, v) != SCC_OK) continue;
+            if (b->nbig == 0) continue;
+            float ms = 0.f;
+            rc = time_it(&ms);
+            if (rc != SCC_OK) return rc;
+            if (ms < best) { best = ms; bc = c; bb = v; }
+        }
+    }
+    rc = scc_batch_set_cluster(b, bc, bb);
     if (best_threads) *best_threads = bt;
     if (best_qcap) *best_qcap = bq;
     if (best_ms) *best_ms = best / 2.f;

@@ -27,7 +27,13 @@ struct BatchParams {
     BatchRes *res;
     char *scratch;              // ncta slices of scratch_per_cta bytes
     unsigned long long scratch_per_cta;
-    unsigned *next;             // work counter, zero before the launch
+    unsigned *next;             // work counters next[0] (cluster graphs), next[1] (CTA graphs), zero before the launch
+    uint32_t nbig;              // the first nbig graphs of order run on whole clusters
+    unsigned *cbar;             // per-cluster software barrier counters (check mode), or nullptr
+    uint32_t lead_div;          // a cluster graph uses slice (rank-0 CTA index) / lead_div: 1, or the
+                                // cluster size when every graph of the launch is a cluster graph
+    unsigned *done;             // optional per-graph completion flags (page-locked host memory): set to 1
+                                // after the graph's labels and result are visible to the host
     uint32_t qcap, bu_k;
     int t1, t2, lw;
     unsigned long long timeout_ns;
@@ -35,7 +41,13 @@ struct BatchParams {
 
 // Shared memory of the batch kernel for a CTA size and staging slice.
 size_t sccb_batch_smem(int threads, uint32_t qcap);
-// Resident CTAs of the batch kernel on a device with nsm SMs.
-int sccb_batch_ctas(int threads, uint32_t qcap, int nsm, uint32_t *out);
-// Launch of the batch kernel (the caller zeroes p.next first).
-int sccb_batch_launch(const BatchParams &p, int threads, bool hong, uint32_t ncta, cudaStream_t st);
+// Resident CTAs of the batch kernel on a device with nsm SMs, launched in
+// clusters of `cluster` CTAs (1: no clusters; above 8 needs the non-portable
+// cluster size, which this sets).
+int sccb_batch_ctas(int threads, uint32_t qcap, int nsm, uint32_t *out, int cluster = 1);
+// Launch of the batch kernel (the caller zeroes p.next[0..1] first).
+int sccb_batch_launch(const BatchParams &p, int threads, bool hong, uint32_t ncta, cudaStream_t st, int cluster = 1);
+// CTAs of a launch: at most `resident`, a whole number of clusters.
+uint32_t sccb_launch_ctas(uint32_t resident, uint32_t n, uint32_t nbig, int cluster);
+// Processing order (cluster graphs first, each part largest first); returns nbig.
+uint32_t sccb_order(const BatchGraph *g, uint32_t n, uint32_t big_vertices, int cluster, uint32_t *order);

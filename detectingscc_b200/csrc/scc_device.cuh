@@ -246,6 +246,88 @@ struct BlockExec {
     }
 };
 
+__device__ __forceinline__ unsigned cluster_rank()
+{
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ unsigned cluster_size()
+{
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+    return r;
+}
+// Hardware cluster barrier (every thread of every CTA of the cluster);
+// writes before it, in any state space, are visible to the whole cluster
+// after it.
+__device__ __forceinline__ void cluster_barrier()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// One graph on the CTAs of a thread-block cluster (co-scheduled by the
+// hardware, so the barrier is the cluster barrier and needs no timeout).
+// The error word is read between two barriers: no pass body runs while
+// any CTA reads it, so every CTA takes the same branch.
+//
+// With `soft` set, the barrier is instead a counter in global memory (the
+// grid barrier's bit-flip scheme over the cluster's CTAs) whose waits give
+// up after soft_timeout_ns with E_TIMEOUT: a check mode in which a
+// mismatch of barrier counts between the CTAs ends in an error status
+// rather than a wait that never ends.
+template <bool INSTR>
+struct ClusterExec {
+    static constexpr bool instr = INSTR;
+    static constexpr bool grid = false;
+    Ctl *ctl;
+    unsigned gl;
+    unsigned rank, csize;
+    unsigned *soft;   // the cluster's barrier counter, or nullptr for the hardware barrier
+    unsigned long long soft_timeout_ns;
+    __device__ __forceinline__ unsigned tid() const { return rank * blockDim.x + threadIdx.x; }
+    __device__ __forceinline__ unsigned nthr() const { return csize * blockDim.x; }
+    __device__ __forceinline__ unsigned wid() const { return tid() >> 5; }
+    __device__ __forceinline__ unsigned nwarps() const { return nthr() >> 5; }
+    __device__ __forceinline__ bool leader() const { return rank == 0 && threadIdx.x == 0; }
+    __device__ void barrier()
+    {
+        if (!soft) {
+            cluster_barrier();
+            return;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const unsigned nb = rank == 0 ? (0x80000000u - (csize - 1u)) : 1u;
+            unsigned old;
+            asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(soft), "r"(nb) : "memory");
+            unsigned long long t0 = 0;
+            for (unsigned spin = 0;; spin++) {
+                unsigned v;
+                asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(soft) : "memory");
+                if (((v ^ old) & 0x80000000u) != 0u) break;
+                if ((spin & 255u) == 0u) {
+                    const unsigned long long t = gtimer();
+                    if (spin == 0) t0 = t;
+                    else if (t - t0 > soft_timeout_ns) {
+                        set_error(ctl, E_TIMEOUT, 1001);
+                        break;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+    __device__ bool sync()
+    {
+        __shared__ int s_err;
+        barrier();
+        if (threadIdx.x == 0) s_err = *(volatile int *)&ctl->error;
+        barrier();
+        return s_err == 0;
+    }
+};
+
 // One pass: clear the counters the pass after next will push into, run the
 // body with (cur, nxt) counter slots, then the barrier.  A pass pushes into
 // counter slot gl%3 and buffer parity gl&1; the following pass reads them as

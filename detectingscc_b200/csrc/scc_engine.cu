@@ -136,19 +136,41 @@ void *pick_block(bool instr, bool hong)
 
 }  // namespace
 
-int scc_ctx_reserve(scc_context *ctx, uint32_t V, uint32_t E)
+namespace {
+
+// Offsets of the whole-graph workspace (all 256-byte aligned).
+struct WsLayout {
+    size_t st, label, stamp, smin, L0, L1, Q[4], H[4], piv, ctl, need, hcap;
+};
+
+WsLayout ws_layout(uint32_t V, uint32_t E)
 {
-    const size_t hcap = (size_t)E / CH + (size_t)E / HEAVY_T + 64;
+    WsLayout o{};
+    o.hcap = (size_t)E / CH + (size_t)E / HEAVY_T + 64;
     const size_t n1 = (size_t)V + 1;
     size_t need = 0;
     auto take = [&](size_t bytes) { size_t off = need; need = align_up(need + bytes, 256); return off; };
-    size_t o_st = take(n1 * 4), o_label = take(n1 * 4), o_stamp = take(n1 * 4), o_smin = take(n1 * 4);
-    size_t o_L0 = take(n1 * 4), o_L1 = take(n1 * 4);
-    size_t o_Q[4], o_H[4];
-    for (int i = 0; i < 4; i++) o_Q[i] = take(n1 * 4);
-    for (int i = 0; i < 4; i++) o_H[i] = take(hcap * sizeof(uint2));
-    size_t o_piv = take((4 * n1 + 8) * 8);
-    size_t o_ctl = take(sizeof(Ctl));
+    o.st = take(n1 * 4); o.label = take(n1 * 4); o.stamp = take(n1 * 4); o.smin = take(n1 * 4);
+    o.L0 = take(n1 * 4); o.L1 = take(n1 * 4);
+    for (int i = 0; i < 4; i++) o.Q[i] = take(n1 * 4);
+    for (int i = 0; i < 4; i++) o.H[i] = take(o.hcap * sizeof(uint2));
+    o.piv = take((4 * n1 + 8) * 8);
+    o.ctl = take(sizeof(Ctl));
+    o.need = need;
+    return o;
+}
+
+}  // namespace
+
+size_t scc_ctx_ws_need(uint32_t V, uint32_t E) { return ws_layout(V, E).need; }
+
+int scc_ctx_reserve(scc_context *ctx, uint32_t V, uint32_t E)
+{
+    const WsLayout o = ws_layout(V, E);
+    const size_t need = o.need, hcap = o.hcap;
+    const size_t o_st = o.st, o_label = o.label, o_stamp = o.stamp, o_smin = o.smin, o_L0 = o.L0, o_L1 = o.L1;
+    const size_t *o_Q = o.Q, *o_H = o.H;
+    const size_t o_piv = o.piv, o_ctl = o.ctl;
     if (need > ctx->ws_bytes) {
         if (ctx->ws) cudaFree(ctx->ws);
         ctx->ws = nullptr;
@@ -406,6 +428,7 @@ extern "C" int scc_set_tuning(scc_context *ctx, const char *key, long long value
     else if (!strcmp(key, "timeout_ms")) ctx->timeout_ms = (uint32_t)value;
     else if (!strcmp(key, "max_blocks_per_sm")) ctx->max_blocks_per_sm = (int)value;
     else if (!strcmp(key, "bu_k")) ctx->bu_k = (uint32_t)value;
+    else if (!strcmp(key, "cluster_check")) ctx->cluster_check = value ? 1 : 0;
     else if (!strcmp(key, "qcap")) {
         if (value < 32 || value > 768) return SCC_ERR_INVALID_ARG;
         ctx->qcap = (uint32_t)value;

@@ -33,6 +33,7 @@ struct scc_context {
     int max_blocks_per_sm = 0;           // 0 = occupancy limit
     uint32_t qcap = 512;                 // per-warp staging slice entries (2 queues x 32 warps in shared memory)
     uint32_t bu_k = 2;                   // bottom-up BFS step when frontier edges > bu_k * scope (0 = off)
+    int cluster_check = 0;               // batched launches: bounded software cluster barriers (check mode)
 
     // optional per-pass trace
     unsigned long long *dtrace = nullptr, *htrace = nullptr;
@@ -42,3 +43,5 @@ struct scc_context {
 };
 
 int scc_ctx_reserve(scc_context *ctx, uint32_t V, uint32_t E);
+// Bytes of the workspace scc_ctx_reserve allocates for a graph.
+size_t scc_ctx_ws_need(uint32_t V, uint32_t E);

@@ -120,7 +120,11 @@ int scc_run(scc_context *ctx, const scc_csr_view *g, int algo, uint32_t flags, i
  *                         bu_k * (vertices the search can reach) (default 2,
  *                         0 = never)
  *   "qcap"                entries of each warp's shared-memory staging slice
- *                         (32..768; 2 queues x 32 warps x qcap x 4 bytes) */
+ *                         (32..768; 2 queues x 32 warps x qcap x 4 bytes)
+ *   "cluster_check"       batched launches with clusters use a software
+ *                         barrier in global memory whose waits end after
+ *                         timeout_ms with SCC_ERR_TIMEOUT (a check mode;
+ *                         default 0: the hardware cluster barrier) */
 int scc_set_tuning(scc_context *ctx, const char *key, long long value);
 
 /* Per-pass trace of the last run (enable with scc_set_tuning(ctx, "trace",
@@ -161,22 +165,29 @@ int scc_run_noalloc(const scc_csr_view *g, int algo, uint32_t flags, int warp_wi
  * buffer for its V labels; both stay owned by the caller and must remain
  * valid until the request's result is polled.  `lanes` worker threads, each
  * with its own stream, take whatever has arrived: a graph above
- * large_vertices alone on the whole-GPU path, otherwise every waiting small
- * graph (up to max_graphs_per_batch) in one batched launch.  Lanes run
- * concurrently, so later arrivals overlap on the device with earlier work.
- * All device memory the server holds stays within budget_bytes; a request
- * that cannot fit even alone gets SCC_ERR_BUDGET.  Zero fields take the
- * defaults shown. */
+ * large_vertices alone, on one thread-block cluster of large_cluster CTAs;
+ * otherwise every waiting small graph (up to max_graphs_per_batch) in one
+ * batched launch, graphs of at least big_vertices vertices on clusters of
+ * `cluster` CTAs and the rest one per CTA.  Lanes run concurrently: copies
+ * and kernels of later arrivals overlap on the device with earlier work,
+ * and no launch needs the whole GPU.  CSR arrays in page-locked memory are
+ * copied by DMA directly; pageable ones go through the lane's page-locked
+ * staging.  All device memory the server holds stays within budget_bytes;
+ * a request that cannot fit even alone gets SCC_ERR_BUDGET.  Zero fields
+ * take the defaults shown. */
 typedef struct {
     uint64_t budget_bytes;          /* 120e9 */
-    uint32_t lanes;                 /* 4 */
+    uint32_t lanes;                 /* 8 */
     uint32_t max_graphs_per_batch;  /* 512 */
     uint32_t large_vertices;        /* 65536 */
-    int32_t batch_threads;          /* 256 (128, 256, 512, 1024) */
-    uint32_t qcap;                  /* 128 */
+    int32_t batch_threads;          /* 1024 (128, 256, 512, 1024) */
+    uint32_t qcap;                  /* 256 (32..768) */
     int32_t algo;                   /* SCC_ALGO_VSLOTA */
     uint32_t flags;                 /* SCC_FLAG_TRIM1 | SCC_FLAG_TRIM2 as wanted (host inputs only) */
     int32_t warp_width;             /* 1 */
+    uint32_t cluster;               /* 4 (1, 2, 4, 8, 16) */
+    uint32_t big_vertices;          /* 16384 */
+    uint32_t large_cluster;         /* 16, or the largest cluster the device holds */
 } scc_server_config;
 
 typedef struct {
@@ -198,6 +209,8 @@ int scc_server_submit(scc_server *s, const scc_csr_view *host_graph, uint32_t *l
 /* Returns up to cap finished results (waits up to wait_ms for one). */
 int scc_server_poll(scc_server *s, scc_server_result *out, uint32_t cap, uint32_t *n, int wait_ms);
 int scc_server_info(scc_server *s, uint64_t *pending, uint64_t *completed, uint64_t *held_bytes, uint64_t *rejected);
+/* Kernel launches the server has made so far. */
+int scc_server_launches(scc_server *s, uint64_t *launches);
 /* Finishes every submitted request, then frees everything. */
 int scc_server_destroy(scc_server *s);
 
@@ -257,7 +270,15 @@ int scc_batch_run(scc_batch *b, int algo, uint32_t flags, int warp_width, uint32
  * per-warp staging slice (32..768 entries). */
 int scc_batch_set_schedule(scc_batch *b, int threads, uint32_t qcap);
 int scc_batch_get_schedule(scc_batch *b, int *threads, uint32_t *qcap);
-/* Times every candidate schedule on the batch and keeps the fastest. */
+/* Thread-block clusters: with cluster > 1 (2, 4, 8, 16) the launch is made of
+ * clusters of that many CTAs, and every graph with at least big_vertices
+ * vertices runs on a whole cluster (the CTAs share one scratch slice and
+ * meet at the hardware cluster barrier), before the remaining graphs run
+ * one per CTA.  cluster 1 (the default) runs every graph on one CTA. */
+int scc_batch_set_cluster(scc_batch *b, int cluster, uint32_t big_vertices);
+int scc_batch_get_cluster(scc_batch *b, int *cluster, uint32_t *big_vertices, uint32_t *num_cluster_graphs);
+/* Times every candidate schedule on the batch and keeps the fastest: CTA
+ * size and staging slice first, then cluster size and big_vertices. */
 int scc_batch_autotune(scc_batch *b, int algo, uint32_t flags, int warp_width, int *best_threads,
                        uint32_t *best_qcap, float *best_ms);
 int scc_batch_info(scc_batch *b, uint64_t *num_vertices, uint64_t *num_edges, uint32_t *num_graphs);

@@ -77,3 +77,33 @@ def test_bad_graph_fails_alone(engine, oracle_lib):
             assert res[i][2] == 0 and np.array_equal(b.labels_of(labels, i), ref[1:])
     finally:
         b.close()
+
+
+@pytest.mark.parametrize("algo,w", [("g", 1), ("h", 1), ("y", 8)])
+def test_cluster_graphs_match_tarjan(engine, oracle_lib, algo, w):
+    """Graphs run on whole thread-block clusters (every cluster size) give
+    the same labels as one CTA per graph and as Tarjan: first with the
+    bounded software cluster barrier (check mode), then the hardware one."""
+    gs = _mix(40, seed=7, vmax=6000)
+    gs.append(scc.graph_from_arcs(1, [], []))
+    ref = [oracle_lib.tarjan(g.V, g.Fr, g.Fc)[0][1:] for g in gs]
+    for check in (1, 0):
+        engine.set_tuning("cluster_check", check)
+        b = scc.Batch(engine, gs)
+        try:
+            base, _, _ = b.run(algo=algo, warp=w)
+            for cl, big in [(2, 0), (4, 1000), (8, 2000), (16, 0)]:
+                b.set_cluster(cl, big)
+                c, bv, nb = b.cluster()
+                assert (c, bv) == (cl, big) and nb == sum(g.V >= big for g in gs)
+                labels, res, _ = b.run(algo=algo, warp=w)
+                assert all(r[2] == 0 for r in res), (check, cl, res)
+                assert np.array_equal(labels, base)
+                for i in range(len(gs)):
+                    assert np.array_equal(b.labels_of(labels, i), ref[i]), (check, cl, big, i)
+            b.set_cluster(1, 0)
+            again, _, _ = b.run(algo=algo, warp=w)
+            assert np.array_equal(again, base)
+        finally:
+            b.close()
+            engine.set_tuning("cluster_check", 0)

@@ -107,3 +107,36 @@ def test_concurrent_submitters():
         assert got == len(small)
     finally:
         srv.close()
+
+
+def test_pinned_and_pageable_inputs_give_the_same_labels():
+    """Page-locked CSR arrays are copied by DMA directly, pageable ones through
+    the lane's staging; both give the solo labels."""
+    import torch
+    small, large = _pool(seed=9)
+
+    def pinned(g):
+        ts = [torch.from_numpy(a.view(np.int32)).pin_memory() for a in (g.Fr, g.Fc, g.Br, g.Bc)]
+        h = scc.Graph(g.V, g.E, *(t.numpy().view(np.uint32) for t in ts))
+        h._pins = ts
+        return h
+
+    eng = scc.Engine(0)
+    alone = [eng.run(g, algo="y").labels.copy() for g in small + [large]]
+    eng.close()
+    srv = scc.Server(0, algo="y", lanes=2, large_vertices=32768)
+    try:
+        tickets = {}
+        for i, g in enumerate(small + [large]):
+            tickets[srv.submit(pinned(g))] = i
+            tickets[srv.submit(g)] = i
+        got = 0
+        t0 = time.time()
+        while got < len(tickets) and time.time() - t0 < 60:
+            for r in srv.poll(64, wait_ms=200):
+                assert r["status"] == 0, r
+                assert np.array_equal(r["labels"], alone[tickets[r["ticket"]]])
+                got += 1
+        assert got == len(tickets)
+    finally:
+        srv.close()
