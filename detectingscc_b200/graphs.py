@@ -175,22 +175,42 @@ def _planted_chain(V: int, deg: float, rng: np.random.Generator) -> Tuple[np.nda
     return np.concatenate(srcs), np.concatenate(dsts)
 
 
+def batch_mix_sizes(n_graphs: int = 4096, vmin: int = 64, vmax: int = 65536, dmin: float = 4.0,
+                    dmax: float = 16.0, seed: int = 1) -> List[Tuple[int, float]]:
+    """(V, mean out-degree) of every graph of the mix, without building any."""
+    out = []
+    for i in range(n_graphs):
+        rng = np.random.default_rng([seed, i])
+        V = int(round(math.exp(rng.uniform(math.log(vmin), math.log(vmax)))))
+        out.append((V, float(rng.uniform(dmin, dmax))))
+    return out
+
+
+def batch_mix_graph(i: int, vmin: int = 64, vmax: int = 65536, dmin: float = 4.0, dmax: float = 16.0,
+                    seed: int = 1) -> Tuple[int, np.ndarray, np.ndarray]:
+    """Graph i of the mix as (V, src, dst) numpy arcs.  Every graph has its
+    own generator (seeded by (seed, i)), so any subset can be built alone."""
+    rng = np.random.default_rng([seed, i])
+    V = int(round(math.exp(rng.uniform(math.log(vmin), math.log(vmax)))))
+    deg = float(rng.uniform(dmin, dmax))
+    if i % 2 == 0:
+        m = int(round(V * deg))
+        s = rng.integers(1, V + 1, m)
+        d = rng.integers(1, V + 1, m)
+    else:
+        s, d = _planted_chain(V, deg, rng)
+    return V, s, d
+
+
+def batch_mix_bytes(V: int, deg: float) -> int:
+    """Estimated forward + reverse CSR bytes of a mix graph (for sharding)."""
+    return 4 * (2 * (V + 2) + 2 * int(round(V * deg)))
+
+
 def batch_mix(n_graphs: int = 4096, vmin: int = 64, vmax: int = 65536, dmin: float = 4.0,
               dmax: float = 16.0, seed: int = 1) -> List[Tuple[int, np.ndarray, np.ndarray]]:
     """List of (V, src, dst) numpy arcs for the batched configuration."""
-    rng = np.random.default_rng(seed)
-    out = []
-    for i in range(n_graphs):
-        V = int(round(math.exp(rng.uniform(math.log(vmin), math.log(vmax)))))
-        deg = float(rng.uniform(dmin, dmax))
-        if i % 2 == 0:
-            m = int(round(V * deg))
-            s = rng.integers(1, V + 1, m)
-            d = rng.integers(1, V + 1, m)
-        else:
-            s, d = _planted_chain(V, deg, rng)
-        out.append((V, s, d))
-    return out
+    return [batch_mix_graph(i, vmin, vmax, dmin, dmax, seed) for i in range(n_graphs)]
 
 
 def random_graph(V: int, m: int, seed: int = 0) -> Tuple[int, np.ndarray, np.ndarray]:
