@@ -175,6 +175,22 @@ __device__ __forceinline__ uint32_t guard_id(uint32_t x, uint32_t V, Ctl *c)
 // ---------------------------------------------------------------------
 // execution policies
 // ---------------------------------------------------------------------
+// Per-CTA copy of the counters the last pass pushed (written by thread 0
+// right after the pass barrier, read by every thread through last_count):
+// one load per CTA instead of one per warp on the same few words, which made
+// a same-address hot spot in L2 on every pass.
+__device__ __forceinline__ unsigned *cnt_snap()
+{
+    __shared__ unsigned s_cnt[NCNT];
+    return s_cnt;
+}
+__device__ __forceinline__ void take_snap(const unsigned *c)
+{
+    unsigned *d = cnt_snap();
+#pragma unroll
+    for (int i = 0; i < NCNT; i++) d[i] = *(volatile const unsigned *)&c[i];
+}
+
 template <bool INSTR>
 struct GridExec {
     static constexpr bool instr = INSTR;
@@ -193,7 +209,7 @@ struct GridExec {
     // waiter leaves early when the sticky error word (polled with the
     // counter in one 8-byte load) is set, or after ctl->timeout_ns; any CTA
     // that sees an error returns, and the error stays set for the others.
-    __device__ bool sync()
+    __device__ bool sync(const unsigned *snap = nullptr)
     {
         __shared__ int s_err;
         __syncthreads();
@@ -219,6 +235,7 @@ struct GridExec {
                 }
             }
             s_err = err;
+            if (snap) take_snap(snap);
         }
         __syncthreads();
         return s_err == 0;
@@ -236,11 +253,14 @@ struct BlockExec {
     __device__ __forceinline__ unsigned wid() const { return threadIdx.x >> 5; }
     __device__ __forceinline__ unsigned nwarps() const { return blockDim.x >> 5; }
     __device__ __forceinline__ bool leader() const { return threadIdx.x == 0; }
-    __device__ bool sync()
+    __device__ bool sync(const unsigned *snap = nullptr)
     {
         __shared__ int s_err;
         __syncthreads();
-        if (threadIdx.x == 0) s_err = *(volatile int *)&ctl->error;
+        if (threadIdx.x == 0) {
+            s_err = *(volatile int *)&ctl->error;
+            if (snap) take_snap(snap);
+        }
         __syncthreads();
         return s_err == 0;
     }
@@ -318,11 +338,14 @@ struct ClusterExec {
         }
         __syncthreads();
     }
-    __device__ bool sync()
+    __device__ bool sync(const unsigned *snap = nullptr)
     {
         __shared__ int s_err;
         barrier();
-        if (threadIdx.x == 0) s_err = *(volatile int *)&ctl->error;
+        if (threadIdx.x == 0) {
+            s_err = *(volatile int *)&ctl->error;
+            if (snap) take_snap(snap);
+        }
         barrier();
         return s_err == 0;
     }
@@ -341,12 +364,14 @@ __device__ __forceinline__ bool run_pass(Ex &ex, int phase, F &&body)
         for (int i = 0; i < NCNT; i++) ex.ctl->lc[clr][i] = 0u;
     }
     body(cur, nxt);
-    bool ok = ex.sync();
+    bool ok = ex.sync(ex.ctl->lc[nxt]);
     if (ex.leader() && ex.ctl->trace && ex.gl < ex.ctl->trace_cap) {
         // pass trace: end time and (phase, items pushed) -- the reference's
         // _DEBUG per-phase event timers (scc_WCC.cu:650-672) at pass granularity
+        // (instrumented runs record the running count of adjacency entries scanned instead)
         const unsigned *c = ex.ctl->lc[nxt];
         unsigned long long pushed = (unsigned long long)vld(&c[C_FQ]) + vld(&c[C_BQ]) + vld(&c[C_LIST]);
+        if constexpr (Ex::instr) pushed = *(volatile unsigned long long *)&ex.ctl->t_edges;
         ex.ctl->trace[2 * ex.gl] = gtimer();
         ex.ctl->trace[2 * ex.gl + 1] = (unsigned long long)phase | (pushed << 8);
     }
@@ -354,11 +379,11 @@ __device__ __forceinline__ bool run_pass(Ex &ex, int phase, F &&body)
     return ok;
 }
 
-// Counter value pushed by the pass that just finished.
+// Counter value pushed by the pass that just finished (the CTA's snapshot).
 template <class Ex>
-__device__ __forceinline__ unsigned last_count(const Ex &ex, int which)
+__device__ __forceinline__ unsigned last_count(const Ex &, int which)
 {
-    return vld(&ex.ctl->lc[(ex.gl + 2u) % 3u][which]);
+    return cnt_snap()[which];
 }
 
 // ---------------------------------------------------------------------

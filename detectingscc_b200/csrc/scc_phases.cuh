@@ -446,13 +446,15 @@ __device__ __forceinline__ void bfs_pull_group(Ex &ex, const Graph &g, const Wor
     if (act) { beg = __ldg(&R[v]); end = __ldg(&R[v + 1]); }
     bool found = false;
     unsigned scanned = 0;
-    if (act && end - beg <= 32u) {
-        for (uint32_t e = beg; e < end; e++) {
+    // the lane scans a short list to its end, a long one's first 8 entries
+    const uint32_t lim = end - beg <= 32u ? end : beg + 8u;
+    if (act) {
+        for (; beg < lim; beg++) {
             scanned++;
-            if ((w.st[guard_id(__ldg(&C[e]), g.V, ex.ctl)] & (RMASK | bit)) == want) { found = true; break; }
+            if ((w.st[guard_id(__ldg(&C[beg]), g.V, ex.ctl)] & (RMASK | bit)) == want) { found = true; break; }
         }
     }
-    unsigned hm = __ballot_sync(FULL, act && end - beg > 32u);
+    unsigned hm = __ballot_sync(FULL, act && !found && end > beg);
     while (hm) {
         const unsigned j = __ffs(hm) - 1u;
         hm &= hm - 1u;
@@ -480,6 +482,112 @@ __device__ __forceinline__ void bfs_pull_group(Ex &ex, const Graph &g, const Wor
         count_edges(ex, t);
     }
     bq_push((unsigned)dir, found, v, w.qcap, w.Q[dir][par], &ex.ctl->lc[nxt][C_FQ + dir], g.V, ex.ctl, 19);
+}
+
+// Bottom-up step over vertex ids instead of a list, both directions at once:
+// item k covers ids k*64+1 .. k*64+64, two per lane (coalesced state and
+// offset loads, no list indirection).  Every lane keeps up to four searches
+// in flight (2 ids x forward/backward), each testing two adjacency entries
+// per step, so a lane waits on one round of gathers for all of them.  Lists
+// longer than 32 entries are searched afterwards by the whole warp.  Used
+// when the scope holds most live vertices: a live vertex outside the scope
+// can only find a visited neighbour of its own range if its range is being
+// searched, so pulling it is the same as reaching it top-down.
+template <class Ex>
+__device__ __forceinline__ void bfs_pull_dense(Ex &ex, const Graph &g, const Work &w, bool puf, bool pub,
+                                               uint32_t k, unsigned par, unsigned nxt)
+{
+    constexpr uint32_t MF = RMASK | FVB, MB = RMASK | BVB;
+    uint32_t v[2], s[2], pos[4], end[4], want[4];
+    bool on[4], found[4];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        v[h] = k * 64u + 1u + 32u * (uint32_t)h + lane_id();
+        s[h] = v[h] <= g.V ? w.st[v[h]] : DEAD;
+    }
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const bool live = s[h] != DEAD;
+        const bool nf = puf && live && !(s[h] & FVB);   // forward: a visited in-neighbour
+        const bool nb = pub && live && !(s[h] & BVB);   // backward: a visited out-neighbour
+        pos[2 * h] = nf ? __ldg(&g.Br[v[h]]) : 0u;
+        end[2 * h] = nf ? __ldg(&g.Br[v[h] + 1u]) : 0u;
+        pos[2 * h + 1] = nb ? __ldg(&g.Fr[v[h]]) : 0u;
+        end[2 * h + 1] = nb ? __ldg(&g.Fr[v[h] + 1u]) : 0u;
+        want[2 * h] = (s[h] & RMASK) | FVB;
+        want[2 * h + 1] = (s[h] & RMASK) | BVB;
+    }
+    unsigned scanned = 0;
+    uint32_t lim[4];   // the lane scans a list to its end if it is short, else its first 8 entries
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+        found[t] = false;
+        on[t] = end[t] > pos[t];
+        lim[t] = end[t] - pos[t] <= 32u ? end[t] : pos[t] + 8u;
+    }
+    // by the lane: two entries of every open search per step (a visited
+    // neighbour is usually among the first entries, the lowest ids)
+    while (on[0] || on[1] || on[2] || on[3]) {
+        uint32_t c0[4], c1[4];
+#pragma unroll
+        for (int t = 0; t < 4; t++) {
+            const uint32_t *C = (t & 1) ? g.Fc : g.Bc;
+            c0[t] = on[t] ? __ldg(&C[pos[t]]) : 0u;
+            c1[t] = on[t] && pos[t] + 1u < end[t] ? __ldg(&C[pos[t] + 1u]) : 0u;
+        }
+#pragma unroll
+        for (int t = 0; t < 4; t++) {
+            if (!on[t]) continue;
+            const uint32_t m = (t & 1) ? MB : MF;
+            const uint32_t a = w.st[guard_id(c0[t], g.V, ex.ctl)];
+            const uint32_t b = pos[t] + 1u < end[t] ? w.st[guard_id(c1[t], g.V, ex.ctl)] : DEAD;
+            if constexpr (Ex::instr) scanned += pos[t] + 1u < end[t] ? 2u : 1u;
+            if ((a & m) == want[t] || (b & m) == want[t]) {
+                found[t] = true;
+                on[t] = false;
+            } else {
+                pos[t] += 2u;
+                on[t] = pos[t] < lim[t];
+            }
+        }
+    }
+    // the rest of long lists by the whole warp, one search at a time
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+        unsigned hm = __ballot_sync(FULL, !found[t] && end[t] > pos[t]);
+        const uint32_t *C = (t & 1) ? g.Fc : g.Bc;
+        const uint32_t m = (t & 1) ? MB : MF;
+        while (hm) {
+            const unsigned j = __ffs(hm) - 1u;
+            hm &= hm - 1u;
+            const uint32_t bj = __shfl_sync(FULL, pos[t], j), ej = __shfl_sync(FULL, end[t], j);
+            const uint32_t wj = __shfl_sync(FULL, want[t], j);
+            for (uint32_t b = bj; b < ej; b += 32u) {
+                const uint32_t e = b + lane_id();
+                const bool hit = e < ej && (w.st[guard_id(__ldg(&C[e]), g.V, ex.ctl)] & m) == wj;
+                if constexpr (Ex::instr) scanned += lane_id() == 0 ? min(32u, ej - b) : 0u;
+                if (__ballot_sync(FULL, hit)) {
+                    if (lane_id() == j) found[t] = true;
+                    break;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const uint32_t bits = (found[2 * h] ? FVB : 0u) | (found[2 * h + 1] ? BVB : 0u);
+        if (bits) atomicOr(&w.st[v[h]], bits);
+        // frontier edges of the next level: out-degree forward, in-degree backward
+        if (puf) bq_add_edges(0u, found[2 * h] ? __ldg(&g.Fr[v[h] + 1u]) - __ldg(&g.Fr[v[h]]) : 0u);
+        if (pub) bq_add_edges(1u, found[2 * h + 1] ? __ldg(&g.Br[v[h] + 1u]) - __ldg(&g.Br[v[h]]) : 0u);
+        count_verts(ex, v[h] <= g.V);
+        if (puf) bq_push(0u, found[2 * h], v[h], w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_FQ], g.V, ex.ctl, 19);
+        if (pub) bq_push(1u, found[2 * h + 1], v[h], w.qcap, w.Q[1][par], &ex.ctl->lc[nxt][C_BQ], g.V, ex.ctl, 19);
+    }
+    if constexpr (Ex::instr) {
+        unsigned t = __reduce_add_sync(FULL, scanned);
+        count_edges(ex, t);
+    }
 }
 
 // Seed predicates for the first BFS pass.
@@ -565,14 +673,23 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
         const uint32_t mf = last_count(ex, C_FE), mb = last_count(ex, C_BE);
         const bool puf = w.bu_k && (unsigned long long)mf > (unsigned long long)scope.n * w.bu_k;
         const bool pub = bw && w.bu_k && (unsigned long long)mb > (unsigned long long)scope.n * w.bu_k;
+        // a bottom-up step over most of the live vertices walks the ids
+        // (both directions in one sweep) instead of the scope list
+        const bool dense = (puf || pub) && 2ull * scope.n >= (unsigned long long)g.V;
+        const uint32_t nd = dense ? g.V / 64u + 1u : 0u;
         ok = run_pass(ex, (puf || pub) ? PH_BFS_PULL : PH_BFS, [&](unsigned, unsigned nxt) {
             const unsigned par = ex.gl & 1u, cp = par ^ 1u;
             const uint32_t ngf = (nf + gsz - 1u) / gsz, ngb = (nb + gsz - 1u) / gsz;
-            const uint32_t items_f = puf ? nsg : nhf + ngf;
-            const uint32_t items_b = pub ? nsg : (bw ? nhb + ngb : 0u);
-            for (uint32_t it = ex.wid(); it < items_f + items_b; it += ex.nwarps()) {
-                const int dir = it < items_f ? 0 : 1;
-                const uint32_t k = dir ? it - items_f : it;
+            const uint32_t items_f = puf ? (dense ? 0u : nsg) : nhf + ngf;
+            const uint32_t items_b = pub ? (dense ? 0u : nsg) : (bw ? nhb + ngb : 0u);
+            for (uint32_t it = ex.wid(); it < nd + items_f + items_b; it += ex.nwarps()) {
+                if (it < nd) {
+                    bfs_pull_dense(ex, g, w, puf, pub, it, par, nxt);
+                    continue;
+                }
+                const uint32_t it2 = it - nd;
+                const int dir = it2 < items_f ? 0 : 1;
+                const uint32_t k = dir ? it2 - items_f : it2;
                 if (dir ? pub : puf) {
                     bfs_pull_group(ex, g, w, dir, scope, k, par, nxt);
                     continue;
