@@ -626,6 +626,26 @@ __device__ __forceinline__ unsigned vw_expand(uint32_t beg, uint32_t deg, uint32
     return __reduce_add_sync(FULL, own);
 }
 
+// Minimum of x over the CTA folded into *dst with one atomicMin by thread 0
+// (skipped when *dst is already smaller).  Called by every thread of the
+// CTA; 0xFFFFFFFF means "nothing".  Used where every member found in a pass
+// belongs to the same SCC, so its canonical label needs one atomic per CTA
+// rather than one per warp on the same word.
+__device__ __forceinline__ void block_min_atomic(uint32_t x, uint32_t *dst)
+{
+    __shared__ uint32_t s_min[32];
+    const uint32_t m = __reduce_min_sync(FULL, x);
+    const unsigned wi = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (lane_id() == 0) s_min[wi] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t r = 0xFFFFFFFFu;
+        for (unsigned i = 0; i < nw; i++) r = min(r, s_min[i]);
+        if (r != 0xFFFFFFFFu && r < *(volatile uint32_t *)dst) atomicMin(dst, r);
+    }
+    __syncthreads();
+}
+
 // 64-bit max of a pivot key over the warp, then the CTA; the CTA's thread 0
 // performs one atomicMax.  Called by every thread of the CTA.
 __device__ __forceinline__ void block_max_atomic(unsigned long long key, unsigned long long *dst)

@@ -168,21 +168,23 @@ __device__ bool ph_init(Ex &ex, const Graph &g, const Work &w, bool fold_pivot)
 }
 
 // ---------------------------------------------------------------------
-// trim1, one pass decided on the state before the pass (vSlota / wSlota
-// run trim1 once, scc_Coloring.cu:507-508).  Survivors fold the first-pivot
-// key on the way (pollForFirstPivot, scc_kernels.cu:643-656).
+// init and trim1-once in one sweep (vSlota / wSlota with trim1): with every
+// vertex live in range 0, trim1 is decided by the degrees alone, so the
+// offsets the init pass validates also decide each vertex's first state.
+// Four ids per lane: 128-bit offset loads and 128-bit stores of st, stamp,
+// smin and label.  Survivors are compacted into Lout and bid for the first
+// pivot.  A bad graph sets the error before the barrier, as in ph_init.
 // ---------------------------------------------------------------------
 template <class Ex>
-__device__ bool ph_trim1_once(Ex &ex, const Graph &g, const Work &w, uint32_t *Lout)
+__device__ bool ph_init_trim1(Ex &ex, const Graph &g, const Work &w, uint32_t *Lout)
 {
-    // Runs right after init, when every vertex is live in range 0: a vertex
-    // then has a live same-range in-neighbour iff its in-degree is non-zero
-    // (self-loops count, as in trim1), so the decision reads the offsets
-    // only and the pass can mark vertices as it goes.  Survivors are
-    // compacted into Lout and bid for the first pivot.  Four ids per lane.
     return run_pass(ex, PH_TRIM1_ONCE, [&](unsigned, unsigned nxt) {
+        if (ex.leader() && (g.Fr[0] != 0u || g.Fr[1] != 0u || g.Br[0] != 0u || g.Br[1] != 0u ||
+                            g.Fr[g.V + 1] != g.E || g.Br[g.V + 1] != g.E))
+            set_error(ex.ctl, E_BAD_GRAPH, 62);
         unsigned long long best = 0;
         unsigned ntrim = 0;
+        bool bad = false;
         for (uint32_t base = ex.wid() * 128u; base <= g.V; base += ex.nwarps() * 128u) {
             const uint32_t i0 = base + 4u * lane_id();
             uint32_t f[5], b[5];
@@ -193,28 +195,50 @@ __device__ bool ph_trim1_once(Ex &ex, const Graph &g, const Work &w, uint32_t *L
 #pragma unroll
                 for (int j = 0; j < 5; j++) f[j] = b[j] = 0u;
             }
+            uint32_t st4[4], sm4[4], lb4[4];
 #pragma unroll
             for (int j = 0; j < 4; j++) {
                 const uint32_t v = i0 + (uint32_t)j;
                 const bool valid = v >= 1u && v <= g.V;
                 bool surv = false;
+                st4[j] = DEAD;
+                sm4[j] = DEAD;
+                lb4[j] = v;
+                if (v <= g.V) bad |= f[j] > f[j + 1] || b[j] > b[j + 1];
                 if (valid) {
                     const uint32_t indeg = b[j + 1] - b[j], outdeg = f[j + 1] - f[j];
                     if (indeg == 0u || outdeg == 0u) {
-                        w.st[v] = DEAD;
-                        w.label[v] = v;
-                        w.smin[v] = v;
+                        sm4[j] = v;      // a trimmed vertex is its own SCC
                         ntrim++;
                     } else {
                         surv = true;
+                        st4[j] = 0u;
                         unsigned long long k = ((unsigned long long)(outdeg * indeg) << 32) | (0xFFFFFFFFu - v);
                         best = k > best ? k : best;
                     }
                 }
                 bq_push(0, surv, v, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 10);
             }
+            if (i0 + 3u <= g.V) {
+                *reinterpret_cast<uint4 *>(w.st + i0) = make_uint4(st4[0], st4[1], st4[2], st4[3]);
+                *reinterpret_cast<uint4 *>(w.stamp + i0) = make_uint4(0u, 0u, 0u, 0u);
+                *reinterpret_cast<uint4 *>(w.smin + i0) = make_uint4(sm4[0], sm4[1], sm4[2], sm4[3]);
+                *reinterpret_cast<uint4 *>(w.label + i0) = make_uint4(lb4[0], lb4[1], lb4[2], lb4[3]);
+            } else {
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const uint32_t i = i0 + (uint32_t)j;
+                    if (i <= g.V) {
+                        w.st[i] = st4[j];
+                        w.stamp[i] = 0u;
+                        w.smin[i] = sm4[j];
+                        w.label[i] = lb4[j];
+                    }
+                }
+            }
             count_verts_n(ex, i0 <= g.V ? min(4u, g.V + 1u - i0) : 0u);
         }
+        if (bad) set_error(ex.ctl, E_BAD_GRAPH, 61);
         ntrim = __reduce_add_sync(FULL, ntrim);
         if (lane_id() == 0 && ntrim) atomicAdd(&ex.ctl->n_trim1, (unsigned long long)ntrim);
         block_max_atomic(best, &w.pivkey[0]);
@@ -258,24 +282,25 @@ __device__ bool ph_trim1_fix(Ex &ex, const Graph &g, const Work &w, VList src0, 
                 count_verts(ex, valid);
                 unsigned m = __ballot_sync(FULL, trim);
                 if (lane_id() == 0 && m) atomicAdd(&ex.ctl->n_trim1, (unsigned long long)__popc(m));
-                while (m) {
-                    unsigned j = __ffs(m) - 1u;
-                    m &= m - 1u;
-                    uint32_t vj = __shfl_sync(FULL, v, j), rj = __shfl_sync(FULL, r, j);
+                if (m == 0u) continue;
+                // queue the live same-range neighbours of the trimmed vertices
+                // (they lost an in- or out-neighbour): the warp walks all their
+                // lists together, 64 entries per step
+                auto fn2 = [&](bool v0, uint32_t u0, uint32_t r0, bool v1, uint32_t u1, uint32_t r1) {
+                    if (v0) u0 = guard_id(u0, g.V, ex.ctl);
+                    if (v1) u1 = guard_id(u1, g.V, ex.ctl);
+                    const bool p0 = v0 && (w.st[u0] & RMASK) == r0 && stamp_claim(w.stamp, u0, tag);
+                    const bool p1 = v1 && (w.st[u1] & RMASK) == r1 && stamp_claim(w.stamp, u1, tag);
+                    bq_push(0, p0, u0, w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_FQ], g.V, ex.ctl, 11);
+                    bq_push(0, p1, u1, w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_FQ], g.V, ex.ctl, 11);
+                };
 #pragma unroll
-                    for (int dir = 0; dir < 2; dir++) {
-                        const uint32_t *R = dir ? g.Br : g.Fr;
-                        const uint32_t *C = dir ? g.Bc : g.Fc;
-                        uint32_t beg = __ldg(&R[vj]), end = __ldg(&R[vj + 1]);
-                        for (uint32_t b = beg; b < end; b += 32u) {
-                            uint32_t e = b + lane_id();
-                            bool ok2 = e < end, push = false;
-                            uint32_t u = ok2 ? guard_id(__ldg(&C[e]), g.V, ex.ctl) : 0u;
-                            if (ok2 && (w.st[u] & RMASK) == rj) push = stamp_claim(w.stamp, u, tag);
-                            bq_push(0, push, u, w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_FQ], g.V, ex.ctl, 11);
-                        }
-                        count_edges(ex, end - beg);
-                    }
+                for (int dir = 0; dir < 2; dir++) {
+                    const uint32_t *R = dir ? g.Br : g.Fr;
+                    const uint32_t *C = dir ? g.Bc : g.Fc;
+                    const uint32_t beg = trim ? __ldg(&R[v]) : 0u;
+                    const uint32_t deg = trim ? __ldg(&R[v + 1]) - beg : 0u;
+                    count_edges(ex, lbs_expand2(beg, deg, r, C, fn2));
                 }
             }
             bq_flush(1, w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_FQ], nullptr, nullptr, g.V, ex.ctl);
@@ -630,16 +655,22 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
                 atomicOr(&w.st[p], bits);
                 atomicAdd(&ex.ctl->n_pivot, 1ull);
             }
+            // 64-entry pieces, one per warp, so the hub's lists spread over
+            // the whole grid in one round of gathers
             const uint32_t r = w.st[p] & RMASK;
-            const uint32_t nfc = (__ldg(&g.Fr[p + 1]) - __ldg(&g.Fr[p]) + CH - 1u) / CH;
-            const uint32_t nbc = bw ? (__ldg(&g.Br[p + 1]) - __ldg(&g.Br[p]) + CH - 1u) / CH : 0u;
+            const uint32_t fb = __ldg(&g.Fr[p]), fe = __ldg(&g.Fr[p + 1]);
+            const uint32_t bb = bw ? __ldg(&g.Br[p]) : 0u, be = bw ? __ldg(&g.Br[p + 1]) : 0u;
+            const uint32_t nfc = (fe - fb + 63u) / 64u, nbc = (be - bb + 63u) / 64u;
             for (uint32_t c = ex.wid(); c < nfc + nbc; c += ex.nwarps()) {
                 const int dir = c < nfc ? 0 : 1;
-                const uint2 hc = make_uint2(p, dir ? c - nfc : c);
-                auto fn2 = [&](bool v0, uint32_t n0, uint32_t r0, bool v1, uint32_t n1, uint32_t r1) {
-                    bfs_edge_visit2(ex, g, w, dir, v0, n0, r0, v1, n1, r1, par, nxt);
-                };
-                chunk_expand(ex, dir ? g.Br : g.Fr, dir ? g.Bc : g.Fc, hc, r, fn2);
+                const uint32_t beg = dir ? bb + (c - nfc) * 64u : fb + c * 64u;
+                const uint32_t end = min(beg + 64u, dir ? be : fe);
+                const uint32_t *C = dir ? g.Bc : g.Fc;
+                const uint32_t e0 = beg + lane_id(), e1 = e0 + 32u;
+                const bool v0 = e0 < end, v1 = e1 < end;
+                const uint32_t n0 = v0 ? __ldg(&C[e0]) : 0u, n1 = v1 ? __ldg(&C[e1]) : 0u;
+                bfs_edge_visit2(ex, g, w, dir, v0, n0, r, v1, n1, r, par, nxt);
+                count_edges(ex, end - beg);
             }
         }
         for (uint32_t it = ex.wid(); it < ng; it += ex.nwarps()) {
@@ -807,6 +838,7 @@ __device__ bool ph_hong_update(Ex &ex, const Graph &g, const Work &w, VList src,
                                bool single, bool fold)
 {
     return run_pass(ex, PH_HONG_UPDATE, [&](unsigned, unsigned nxt) {
+        uint32_t mn = 0xFFFFFFFFu;   // single: smallest member of the pivot's SCC seen by this thread
         for (uint32_t base = ex.wid() * 128u; base < src.n; base += ex.nwarps() * 128u) {
             uint32_t v[4], s[4];
             bool ok[4];
@@ -829,12 +861,14 @@ __device__ bool ph_hong_update(Ex &ex, const Graph &g, const Work &w, VList src,
                         surv = true;
                     }
                 }
-                smin_fold(scc, p, v[j], w.smin);
+                if (single) mn = scc ? min(mn, v[j]) : mn;
+                else smin_fold(scc, p, v[j], w.smin);
                 bq_push(0, surv, v[j], w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 15);
                 if (fold) range_max_atomic(surv, nr, surv ? pivot_key(g, v[j]) : 0ull, w.pivkey);
             }
             count_verts_n(ex, (unsigned)ok[0] + ok[1] + ok[2] + ok[3]);
         }
+        if (single) block_min_atomic(mn, w.pivkey[0] ? &w.smin[key_vertex(w.pivkey[0])] : w.smin);
         bq_flush(1, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], nullptr, nullptr, g.V, ex.ctl);
     });
 }
@@ -847,6 +881,7 @@ __device__ bool ph_slota_first_update(Ex &ex, const Graph &g, const Work &w, VLi
 {
     return run_pass(ex, PH_SLOTA_FIRST_UPDATE, [&](unsigned, unsigned nxt) {
         const uint32_t p = key_vertex(w.pivkey[0]);
+        uint32_t mn = 0xFFFFFFFFu;   // smallest member of p's SCC seen by this thread
         for (uint32_t base = ex.wid() * 128u; base < src.n; base += ex.nwarps() * 128u) {
             uint32_t v[4], s[4];
             bool ok[4];
@@ -860,11 +895,12 @@ __device__ bool ph_slota_first_update(Ex &ex, const Graph &g, const Work &w, VLi
                     if ((s[j] & FVB) && (s[j] & BVB)) { w.st[v[j]] = DEAD; w.label[v[j]] = p; scc = true; }
                     else { w.st[v[j]] = v[j]; surv = true; }
                 }
-                smin_fold(scc, p, v[j], w.smin);
+                mn = scc ? min(mn, v[j]) : mn;
                 bq_push(0, surv, v[j], w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 16);
             }
             count_verts_n(ex, (unsigned)ok[0] + ok[1] + ok[2] + ok[3]);
         }
+        block_min_atomic(mn, w.pivkey[0] ? &w.smin[p] : w.smin);   // mn stays 0xFFFFFFFF without a pivot
         bq_flush(1, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], nullptr, nullptr, g.V, ex.ctl);
     });
 }
@@ -1055,10 +1091,11 @@ template <class Ex>
 __device__ int slota_front(Ex &ex, const Graph &g, const Work &w, bool t1, int lw, Carry &cy)
 {
     VList scope{nullptr, g.V, 1u};
-    if (!ph_init(ex, g, w, !t1)) return RUN_ERROR;
     if (t1) {
-        if (!ph_trim1_once(ex, g, w, w.L[0])) return RUN_ERROR;
+        if (!ph_init_trim1(ex, g, w, w.L[0])) return RUN_ERROR;
         scope = VList{w.L[0], last_count(ex, C_LIST), 0u};
+    } else if (!ph_init(ex, g, w, true)) {
+        return RUN_ERROR;
     }
     if (!first_fwbw(ex, g, w, lw, scope)) return RUN_ERROR;
     if (!ph_slota_first_update(ex, g, w, scope, w.L[1])) return RUN_ERROR;
