@@ -26,7 +26,7 @@ struct scc_context {
     size_t capV = 0, capE = 0;
 
     // tuning
-    uint32_t tail_vertices = 4096;       // CTA 0 finishes alone at or below this live count
+    uint32_t tail_vertices = 1024;       // CTA 0 finishes alone at or below this live count
     uint32_t block_max_vertices = 16384; // graphs up to this size run on one CTA
     uint32_t block_max_edges = 262144;
     uint32_t timeout_ms = 4000;          // bound on any single grid-barrier wait

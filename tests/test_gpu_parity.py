@@ -90,7 +90,7 @@ def test_tail_switch_to_one_cta(engine, oracle_lib):
                     # CTA 0 takes over at the first main-loop iteration / peel
                     assert res.stats["outer_iters"] == 0 or res.stats["tail_pass"] > 0
     finally:
-        engine.set_tuning("tail_vertices", 4096)
+        engine.set_tuning("tail_vertices", 1024)
 
 
 def test_repeatable(engine, oracle_lib):
