@@ -449,87 +449,32 @@ __device__ __forceinline__ void chunk_expand(Ex &ex, const uint32_t *__restrict_
     count_edges(ex, end > beg ? end - beg : 0u);
 }
 
-// Bottom-up step for one direction over 32 scope vertices (Beamer's
-// direction-optimizing BFS): an unvisited live vertex looks for a visited
-// neighbour of its own range among its in-neighbours (forward search) or
-// out-neighbours (backward search) and stops at the first one.  Lists up to
-// 32 entries are scanned by their lane; longer ones by the whole warp.
+// Bottom-up step over 64 vertices, both directions at once: entries
+// k*64 .. k*64+63 of `src` (the scope list, or the id range 1..V when the
+// scope holds most live vertices: coalesced state and offset loads, no list
+// indirection), two per lane.  Every lane keeps up to four searches in
+// flight (2 vertices x forward/backward), each testing two adjacency
+// entries per step, so a lane waits on one round of gathers for all of
+// them; a list longer than 32 entries gets its first 8 entries tested by
+// the lane (a visited neighbour is usually among the first, lowest ids) and
+// the rest by the whole warp.  A live vertex outside the scope can only
+// find a visited neighbour of its own range if its range is being
+// searched, so walking ids reaches the same set as walking the scope.
 template <class Ex>
-__device__ __forceinline__ void bfs_pull_group(Ex &ex, const Graph &g, const Work &w, int dir, VList scope,
-                                               uint32_t k, unsigned par, unsigned nxt)
-{
-    const uint32_t bit = dir ? BVB : FVB;
-    const uint32_t *R = dir ? g.Fr : g.Br;
-    const uint32_t *C = dir ? g.Fc : g.Bc;
-    const uint32_t i = k * 32u + lane_id();
-    const bool valid = i < scope.n;
-    const uint32_t v = valid ? scope.at(i) : 0u;
-    const uint32_t s = valid ? w.st[v] : DEAD;
-    const bool act = valid && s != DEAD && !(s & bit);
-    const uint32_t want = (s & RMASK) | bit;
-    uint32_t beg = 0, end = 0;
-    if (act) { beg = __ldg(&R[v]); end = __ldg(&R[v + 1]); }
-    bool found = false;
-    unsigned scanned = 0;
-    // the lane scans a short list to its end, a long one's first 8 entries
-    const uint32_t lim = end - beg <= 32u ? end : beg + 8u;
-    if (act) {
-        for (; beg < lim; beg++) {
-            scanned++;
-            if ((w.st[guard_id(__ldg(&C[beg]), g.V, ex.ctl)] & (RMASK | bit)) == want) { found = true; break; }
-        }
-    }
-    unsigned hm = __ballot_sync(FULL, act && !found && end > beg);
-    while (hm) {
-        const unsigned j = __ffs(hm) - 1u;
-        hm &= hm - 1u;
-        const uint32_t bj = __shfl_sync(FULL, beg, j), ej = __shfl_sync(FULL, end, j);
-        const uint32_t wj = __shfl_sync(FULL, want, j);
-        for (uint32_t b = bj; b < ej; b += 32u) {
-            const uint32_t e = b + lane_id();
-            const bool ok = e < ej;
-            const bool hit = ok && (w.st[guard_id(__ldg(&C[e]), g.V, ex.ctl)] & (RMASK | bit)) == wj;
-            if (lane_id() == 0) scanned += min(32u, ej - b);
-            if (__ballot_sync(FULL, hit)) {
-                if (lane_id() == j) found = true;
-                break;
-            }
-        }
-    }
-    if (found) atomicOr(&w.st[v], bit);
-    {
-        const uint32_t *Rn = dir ? g.Br : g.Fr;
-        bq_add_edges((unsigned)dir, found ? __ldg(&Rn[v + 1]) - __ldg(&Rn[v]) : 0u);
-    }
-    count_verts(ex, valid);
-    if constexpr (Ex::instr) {
-        unsigned t = __reduce_add_sync(FULL, scanned);
-        count_edges(ex, t);
-    }
-    bq_push((unsigned)dir, found, v, w.qcap, w.Q[dir][par], &ex.ctl->lc[nxt][C_FQ + dir], g.V, ex.ctl, 19);
-}
-
-// Bottom-up step over vertex ids instead of a list, both directions at once:
-// item k covers ids k*64+1 .. k*64+64, two per lane (coalesced state and
-// offset loads, no list indirection).  Every lane keeps up to four searches
-// in flight (2 ids x forward/backward), each testing two adjacency entries
-// per step, so a lane waits on one round of gathers for all of them.  Lists
-// longer than 32 entries are searched afterwards by the whole warp.  Used
-// when the scope holds most live vertices: a live vertex outside the scope
-// can only find a visited neighbour of its own range if its range is being
-// searched, so pulling it is the same as reaching it top-down.
-template <class Ex>
-__device__ __forceinline__ void bfs_pull_dense(Ex &ex, const Graph &g, const Work &w, bool puf, bool pub,
-                                               uint32_t k, unsigned par, unsigned nxt)
+__device__ __forceinline__ void bfs_pull2(Ex &ex, const Graph &g, const Work &w, bool puf, bool pub, VList src,
+                                          uint32_t k, unsigned par, unsigned nxt)
 {
     constexpr uint32_t MF = RMASK | FVB, MB = RMASK | BVB;
     uint32_t v[2], s[2], pos[4], end[4], want[4];
-    bool on[4], found[4];
+    bool on[4], found[4], ok[2];
 #pragma unroll
     for (int h = 0; h < 2; h++) {
-        v[h] = k * 64u + 1u + 32u * (uint32_t)h + lane_id();
-        s[h] = v[h] <= g.V ? w.st[v[h]] : DEAD;
+        const uint32_t i = k * 64u + 32u * (uint32_t)h + lane_id();
+        ok[h] = i < src.n;
+        v[h] = ok[h] ? src.at(i) : 0u;
     }
+#pragma unroll
+    for (int h = 0; h < 2; h++) s[h] = ok[h] ? w.st[v[h]] : DEAD;
 #pragma unroll
     for (int h = 0; h < 2; h++) {
         const bool live = s[h] != DEAD;
@@ -605,7 +550,7 @@ __device__ __forceinline__ void bfs_pull_dense(Ex &ex, const Graph &g, const Wor
         // frontier edges of the next level: out-degree forward, in-degree backward
         if (puf) bq_add_edges(0u, found[2 * h] ? __ldg(&g.Fr[v[h] + 1u]) - __ldg(&g.Fr[v[h]]) : 0u);
         if (pub) bq_add_edges(1u, found[2 * h + 1] ? __ldg(&g.Br[v[h] + 1u]) - __ldg(&g.Br[v[h]]) : 0u);
-        count_verts(ex, v[h] <= g.V);
+        count_verts(ex, ok[h]);
         if (puf) bq_push(0u, found[2 * h], v[h], w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_FQ], g.V, ex.ctl, 19);
         if (pub) bq_push(1u, found[2 * h + 1], v[h], w.qcap, w.Q[1][par], &ex.ctl->lc[nxt][C_BQ], g.V, ex.ctl, 19);
     }
@@ -693,7 +638,6 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
                  &ex.ctl->lc[nxt][C_FE], &ex.ctl->lc[nxt][C_BE]);
     });
     if (!ok) return false;
-    const uint32_t nsg = (scope.n + 31u) / 32u;
     for (unsigned lev = 1;; lev++) {
         const uint32_t nf = last_count(ex, C_FQ), nb = last_count(ex, C_BQ);
         const uint32_t nhf = last_count(ex, C_FH), nhb = last_count(ex, C_BH);
@@ -704,27 +648,23 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
         const uint32_t mf = last_count(ex, C_FE), mb = last_count(ex, C_BE);
         const bool puf = w.bu_k && (unsigned long long)mf > (unsigned long long)scope.n * w.bu_k;
         const bool pub = bw && w.bu_k && (unsigned long long)mb > (unsigned long long)scope.n * w.bu_k;
-        // a bottom-up step over most of the live vertices walks the ids
-        // (both directions in one sweep) instead of the scope list
-        const bool dense = (puf || pub) && 2ull * scope.n >= (unsigned long long)g.V;
-        const uint32_t nd = dense ? g.V / 64u + 1u : 0u;
+        // bottom-up steps (both directions in one sweep of 64-vertex items)
+        // walk the ids instead of the scope list when it holds most of them
+        const VList psrc = 2ull * scope.n >= (unsigned long long)g.V ? VList{nullptr, g.V, 1u} : scope;
+        const uint32_t nd = (puf || pub) ? (psrc.n + 63u) / 64u : 0u;
         ok = run_pass(ex, (puf || pub) ? PH_BFS_PULL : PH_BFS, [&](unsigned, unsigned nxt) {
             const unsigned par = ex.gl & 1u, cp = par ^ 1u;
             const uint32_t ngf = (nf + gsz - 1u) / gsz, ngb = (nb + gsz - 1u) / gsz;
-            const uint32_t items_f = puf ? (dense ? 0u : nsg) : nhf + ngf;
-            const uint32_t items_b = pub ? (dense ? 0u : nsg) : (bw ? nhb + ngb : 0u);
+            const uint32_t items_f = puf ? 0u : nhf + ngf;
+            const uint32_t items_b = pub ? 0u : (bw ? nhb + ngb : 0u);
             for (uint32_t it = ex.wid(); it < nd + items_f + items_b; it += ex.nwarps()) {
                 if (it < nd) {
-                    bfs_pull_dense(ex, g, w, puf, pub, it, par, nxt);
+                    bfs_pull2(ex, g, w, puf, pub, psrc, it, par, nxt);
                     continue;
                 }
                 const uint32_t it2 = it - nd;
                 const int dir = it2 < items_f ? 0 : 1;
                 const uint32_t k = dir ? it2 - items_f : it2;
-                if (dir ? pub : puf) {
-                    bfs_pull_group(ex, g, w, dir, scope, k, par, nxt);
-                    continue;
-                }
                 const uint32_t nh = dir ? nhb : nhf;
                 if (k < nh) {
                     uint2 hc = w.H[dir][cp][k];
