@@ -59,6 +59,7 @@ struct __align__(128) Ctl {
     unsigned long long t_start;                    // %globaltimer at kernel entry
     unsigned long long *trace;                     // optional: 2 words per pass
     unsigned trace_cap;
+    unsigned labels_done;                          // the SCC kernel wrote the canonical labels itself
 };
 
 // Phase ids recorded in the pass trace.
@@ -623,6 +624,28 @@ __device__ __forceinline__ unsigned vw_expand(uint32_t beg, uint32_t deg, uint32
         fn(valid, nbr, aux);
     }
     unsigned own = (sub == 0u) ? deg : 0u;
+    return __reduce_add_sync(FULL, own);
+}
+
+// Virtual-warp expansion of two vertices per group at once (the same W
+// lanes per vertex as vw_expand): both lists are walked in the same steps,
+// so every lane has two gathers in flight.  fn(vA, nA, auxA, vB, nB, auxB).
+template <class Fn>
+__device__ __forceinline__ unsigned vw_expand2(uint32_t begA, uint32_t degA, uint32_t auxA, uint32_t begB,
+                                               uint32_t degB, uint32_t auxB, unsigned lw,
+                                               const uint32_t *__restrict__ C, Fn &&fn)
+{
+    const unsigned W = 1u << lw;
+    const unsigned sub = lane_id() & (W - 1u);
+    const unsigned maxd = __reduce_max_sync(FULL, max(degA, degB));
+    for (unsigned base = 0; base < maxd; base += W) {
+        const unsigned k = base + sub;
+        const bool va = k < degA, vb = k < degB;
+        const uint32_t na = va ? __ldg(&C[begA + k]) : 0u;
+        const uint32_t nb = vb ? __ldg(&C[begB + k]) : 0u;
+        fn(va, na, auxA, vb, nb, auxB);
+    }
+    const unsigned own = (sub == 0u) ? degA + degB : 0u;
     return __reduce_add_sync(FULL, own);
 }
 

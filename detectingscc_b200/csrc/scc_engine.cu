@@ -28,7 +28,20 @@ struct Params {
     Work w;
     int t1, t2, lw;
     uint32_t tail_n;
+    uint32_t *out;      // canonical labels (device, V entries) written at the end of the run, or nullptr
 };
+
+// Canonical labels of vertices tid+1, tid+1+n, ...: every vertex takes the
+// smallest member id of its SCC, which the update passes fold into
+// smin[representative].  Runs after the last pass barrier, so label and
+// smin are final.
+__device__ __forceinline__ void write_labels(const Work &w, uint32_t V, uint32_t *out, uint32_t tid, uint32_t n)
+{
+    for (uint32_t v = tid + 1u; v <= V; v += n) {
+        const uint32_t l = w.label[v];
+        out[v - 1u] = l <= V ? w.smin[l] : 0u;
+    }
+}
 
 // ---------------------------------------------------------------------
 // kernels
@@ -62,6 +75,12 @@ __global__ void __launch_bounds__(GRID_THREADS, 1) k_scc_grid(Params p)
         return;
     }
     if (ex.leader()) p.w.ctl->passes = ex.gl;
+    if (rc == RUN_DONE && p.out) {
+        // every CTA is still here: the grid writes the labels (after a switch
+        // to CTA 0 alone, k_canon_write does)
+        write_labels(p.w, p.g.V, p.out, ex.tid(), ex.nthr());
+        if (ex.leader()) p.w.ctl->labels_done = 1u;
+    }
 }
 
 template <bool INSTR, bool HONG>
@@ -73,18 +92,21 @@ __global__ void __launch_bounds__(BLOCK_THREADS, 1) k_scc_block(Params p)
     BlockExec<INSTR> ex{p.w.ctl, 0u};
     Carry cy{0u, 0u, 0u};
     int rc = HONG ? hong_front(ex, p.g, p.w, p.t1, p.t2, p.lw, cy) : slota_front(ex, p.g, p.w, p.t1, p.lw, cy);
-    if (rc == RUN_DONE) {
-        if (HONG) hong_loop(ex, p.g, p.w, cy, 0u);
-        else slota_peels(ex, p.g, p.w, cy, 0u);
-    }
+    if (rc == RUN_DONE) rc = HONG ? hong_loop(ex, p.g, p.w, cy, 0u) : slota_peels(ex, p.g, p.w, cy, 0u);
     if (threadIdx.x == 0) p.w.ctl->passes = ex.gl;
+    if (rc == RUN_DONE && p.out) {
+        write_labels(p.w, p.g.V, p.out, threadIdx.x, blockDim.x);
+        if (threadIdx.x == 0) p.w.ctl->labels_done = 1u;
+    }
 }
 
 // Canonical labels: every vertex takes the smallest member id of its SCC,
 // which the update passes fold into smin[representative].
+// Skipped when the SCC kernel already wrote them (ctl->labels_done).
 __global__ void k_canon_write(const uint32_t *__restrict__ label, const uint32_t *__restrict__ smin,
-                              uint32_t *__restrict__ out, uint32_t V)
+                              uint32_t *__restrict__ out, uint32_t V, const Ctl *ctl)
 {
+    if (ctl && ctl->labels_done) return;
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, n = gridDim.x * blockDim.x;
     for (uint32_t v = tid + 1u; v <= V; v += n) {
         uint32_t l = label[v];
@@ -288,15 +310,32 @@ extern "C" int scc_destroy(scc_context *ctx)
     return SCC_OK;
 }
 
-static int grid_blocks_for(scc_context *ctx, void *fn, size_t smem)
+// Sets the kernel's dynamic shared memory limit (every call: other callers
+// of the same kernel may have set a lower one) and returns the grid of its
+// cooperative launch, computed once per (kernel, shared memory, CTA cap).
+// Returns 0 on failure.
+static int prepare_kernel(scc_context *ctx, void *fn, size_t smem, int threads)
 {
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    for (int i = 0; i < ctx->n_prepared; i++) {
+        const scc_context::Prepared &q = ctx->prepared[i];
+        if (q.fn == fn && q.smem == smem && q.cap == ctx->max_blocks_per_sm) return q.nblocks;
+    }
     int occ = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, GRID_THREADS, smem) != cudaSuccess) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, threads, smem) != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
     if (ctx->max_blocks_per_sm > 0) occ = std::min(occ, ctx->max_blocks_per_sm);
-    return occ * ctx->nsm;
+    const int nb = occ * ctx->nsm;
+    if (nb > 0) {
+        const int slot = ctx->n_prepared < 8 ? ctx->n_prepared++ : 7;
+        ctx->prepared[slot] = scc_context::Prepared{fn, smem, ctx->max_blocks_per_sm, nb};
+    }
+    return nb;
 }
 
 extern "C" int scc_run(scc_context *ctx, const scc_csr_view *gv, int algo, uint32_t flags, int warp_width,
@@ -364,7 +403,8 @@ extern "C" int scc_run(scc_context *ctx, const scc_csr_view *gv, int algo, uint3
     ctx->work.qcap = ctx->qcap;
     ctx->work.bu_k = ctx->bu_k;
     const size_t smem = dyn_smem_bytes(ctx->qcap);
-    Params p{g, ctx->work, (flags & SCC_FLAG_TRIM1) ? 1 : 0, (flags & SCC_FLAG_TRIM2) ? 1 : 0, lw, ctx->tail_vertices};
+    Params p{g, ctx->work, (flags & SCC_FLAG_TRIM1) ? 1 : 0, (flags & SCC_FLAG_TRIM2) ? 1 : 0, lw, ctx->tail_vertices,
+             dout};
     bool use_block = (V <= ctx->block_max_vertices && E <= ctx->block_max_edges);
     if (flags & SCC_FLAG_FORCE_GRID) use_block = false;
     if (flags & SCC_FLAG_FORCE_BLOCK) use_block = true;
@@ -373,13 +413,12 @@ extern "C" int scc_run(scc_context *ctx, const scc_csr_view *gv, int algo, uint3
     CK(cudaEventRecord(ctx->ev[1], st));
     if (use_block) {
         void *fn = pick_block(instr, hong);
-        CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        if (prepare_kernel(ctx, fn, smem, BLOCK_THREADS) <= 0) return SCC_ERR_CUDA;
         void *args[] = {&p};
         CK(cudaLaunchKernel(fn, dim3(1), dim3(BLOCK_THREADS), args, smem, st));
     } else {
         void *fn = pick_grid(instr, hong);
-        CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        nblocks = grid_blocks_for(ctx, fn, smem);
+        nblocks = prepare_kernel(ctx, fn, smem, GRID_THREADS);
         if (nblocks <= 0) return SCC_ERR_CUDA;
         void *args[] = {&p};
         CK(cudaLaunchCooperativeKernel(fn, dim3(nblocks), dim3(GRID_THREADS), args, smem, st));
@@ -388,7 +427,7 @@ extern "C" int scc_run(scc_context *ctx, const scc_csr_view *gv, int algo, uint3
     CK(cudaEventRecord(ctx->ev[2], st));
     if (dout) {
         const int cb = std::min<int>(ctx->nsm * 8, (int)((V + 255) / 256) + 1);
-        k_canon_write<<<cb, 256, 0, st>>>(ctx->work.label, ctx->work.smin, dout, V);
+        k_canon_write<<<cb, 256, 0, st>>>(ctx->work.label, ctx->work.smin, dout, V, ctx->work.ctl);
         launches += 1;
         CK(cudaGetLastError());
         if (!dev) CK(cudaMemcpyAsync(labels_out, dout, (size_t)V * 4, cudaMemcpyDeviceToHost, st));
@@ -479,7 +518,7 @@ int sccb_launch_block_path(const Graph &g, const Work &w, int t1, int t2, int lw
     e = cudaLaunchKernel(fn, dim3(1), dim3(BLOCK_THREADS), args, smem, st);
     if (e != cudaSuccess) return cuda_status(e);
     const int cb = (int)std::min<uint32_t>(1184u, (g.V + 255u) / 256u + 1u);
-    k_canon_write<<<cb, 256, 0, st>>>(w.label, w.smin, dout, g.V);
+    k_canon_write<<<cb, 256, 0, st>>>(w.label, w.smin, dout, g.V, nullptr);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_status(e);
     *launches = 2;

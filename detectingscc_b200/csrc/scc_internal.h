@@ -35,6 +35,12 @@ struct scc_context {
     uint32_t bu_k = 2;                   // bottom-up BFS step when frontier edges > bu_k * scope (0 = off)
     int cluster_check = 0;               // batched launches: bounded software cluster barriers (check mode)
 
+    // grid size of the cooperative launch (occupancy x SMs) per kernel and
+    // shared memory size, computed once
+    struct Prepared { void *fn; size_t smem; int cap; int nblocks; };
+    Prepared prepared[8] = {};
+    int n_prepared = 0;
+
     // optional per-pass trace
     unsigned long long *dtrace = nullptr, *htrace = nullptr;
     uint32_t trace_cap = 0;

@@ -432,6 +432,33 @@ __device__ __forceinline__ void bfs_expand_lanes(Ex &ex, const Graph &g, const W
     count_edges(ex, tot);
 }
 
+// Top-down expansion with the virtual-warp schedule (W = 1 << lw lanes per
+// vertex, the reference's fwd_warp/bwd_warp), two frontier vertices per
+// lane group in the same steps.
+template <class Ex>
+__device__ __forceinline__ void bfs_expand_vw2(Ex &ex, const Graph &g, const Work &w, int dir, uint32_t vA,
+                                               bool actA, uint32_t rA, uint32_t vB, bool actB, uint32_t rB, int lw,
+                                               unsigned par, unsigned nxt)
+{
+    const uint32_t *R = dir ? g.Br : g.Fr;
+    const uint32_t *C = dir ? g.Bc : g.Fc;
+    uint32_t begA = 0, degA = 0, begB = 0, degB = 0;
+    if (actA) { begA = __ldg(&R[vA]); degA = __ldg(&R[vA + 1]) - begA; }
+    if (actB) { begB = __ldg(&R[vB]); degB = __ldg(&R[vB + 1]) - begB; }
+    const bool lead = (lane_id() & ((1u << lw) - 1u)) == 0u;
+    const bool hA = degA > HEAVY_T, hB = degB > HEAVY_T;
+    warp_push_chunks(vA, hA && lead ? (degA + CH - 1u) / CH : 0u, w.H[dir][par], &ex.ctl->lc[nxt][C_FH + dir],
+                     w.hcap, ex.ctl);
+    warp_push_chunks(vB, hB && lead ? (degB + CH - 1u) / CH : 0u, w.H[dir][par], &ex.ctl->lc[nxt][C_FH + dir],
+                     w.hcap, ex.ctl);
+    if (hA) degA = 0u;
+    if (hB) degB = 0u;
+    auto fn2 = [&](bool v0, uint32_t n0, uint32_t r0, bool v1, uint32_t n1, uint32_t r1) {
+        bfs_edge_visit2(ex, g, w, dir, v0, n0, r0, v1, n1, r1, par, nxt);
+    };
+    count_edges(ex, vw_expand2(begA, degA, rA, begB, degB, rB, (unsigned)lw, C, fn2));
+}
+
 // One CH-entry chunk of a heavy vertex, expanded by the whole warp.
 template <class Ex, class Fn>
 __device__ __forceinline__ void chunk_expand(Ex &ex, const uint32_t *__restrict__ R, const uint32_t *__restrict__ C,
@@ -654,7 +681,9 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
         const uint32_t nd = (puf || pub) ? (psrc.n + 63u) / 64u : 0u;
         ok = run_pass(ex, (puf || pub) ? PH_BFS_PULL : PH_BFS, [&](unsigned, unsigned nxt) {
             const unsigned par = ex.gl & 1u, cp = par ^ 1u;
-            const uint32_t ngf = (nf + gsz - 1u) / gsz, ngb = (nb + gsz - 1u) / gsz;
+            // virtual-warp items take two groups of frontier vertices
+            const uint32_t isz = (lw < 0) ? gsz : 2u * gsz;
+            const uint32_t ngf = (nf + isz - 1u) / isz, ngb = (nb + isz - 1u) / isz;
             const uint32_t items_f = puf ? 0u : nhf + ngf;
             const uint32_t items_b = pub ? 0u : (bw ? nhb + ngb : 0u);
             for (uint32_t it = ex.wid(); it < nd + items_f + items_b; it += ex.nwarps()) {
@@ -677,13 +706,23 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
                     const uint32_t gi = k - nh;
                     const uint32_t n = dir ? nb : nf;
                     unsigned slot = (lw < 0) ? lane_id() : (lane_id() >> lw);
-                    uint32_t i = gi * gsz + slot;
+                    uint32_t i = gi * isz + slot;
                     bool valid = i < n;
                     uint32_t v = valid ? w.Q[dir][cp][i] : 0u;
                     uint32_t r = valid ? (w.st[v] & RMASK) : 0u;
                     bool lead = (lw <= 0) || ((lane_id() & ((1u << lw) - 1u)) == 0u);
-                    count_verts(ex, valid && lead);
-                    bfs_expand_lanes(ex, g, w, dir, v, valid, r, lw, par, nxt);
+                    if (lw < 0) {
+                        count_verts(ex, valid && lead);
+                        bfs_expand_lanes(ex, g, w, dir, v, valid, r, lw, par, nxt);
+                    } else {
+                        const uint32_t i2 = i + gsz;
+                        const bool valid2 = i2 < n;
+                        const uint32_t v2 = valid2 ? w.Q[dir][cp][i2] : 0u;
+                        const uint32_t r2 = valid2 ? (w.st[v2] & RMASK) : 0u;
+                        count_verts(ex, valid && lead);
+                        count_verts(ex, valid2 && lead);
+                        bfs_expand_vw2(ex, g, w, dir, v, valid, r, v2, valid2, r2, lw, par, nxt);
+                    }
                 }
             }
             bq_flush(2, w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_FQ], w.Q[1][par], &ex.ctl->lc[nxt][C_BQ], g.V,
