@@ -627,26 +627,36 @@ __device__ __forceinline__ unsigned vw_expand(uint32_t beg, uint32_t deg, uint32
     return __reduce_add_sync(FULL, own);
 }
 
-// Virtual-warp expansion of two vertices per group at once (the same W
-// lanes per vertex as vw_expand): both lists are walked in the same steps,
-// so every lane has two gathers in flight.  fn(vA, nA, auxA, vB, nB, auxB).
-template <class Fn>
-__device__ __forceinline__ unsigned vw_expand2(uint32_t begA, uint32_t degA, uint32_t auxA, uint32_t begB,
-                                               uint32_t degB, uint32_t auxB, unsigned lw,
+// Virtual-warp expansion of K vertices per lane group at once (the same W
+// lanes per vertex as vw_expand): the K lists are walked in the same steps,
+// so every lane has K gathers in flight.  fn(j, valid, nbr) per entry, in
+// pairs of j; returns the entries of the warp.
+template <int K, class Fn>
+__device__ __forceinline__ unsigned vw_expandK(const uint32_t (&beg)[K], const uint32_t (&deg)[K], unsigned lw,
                                                const uint32_t *__restrict__ C, Fn &&fn)
 {
     const unsigned W = 1u << lw;
     const unsigned sub = lane_id() & (W - 1u);
-    const unsigned maxd = __reduce_max_sync(FULL, max(degA, degB));
+    unsigned md = 0, own = 0;
+#pragma unroll
+    for (int j = 0; j < K; j++) {
+        md = max(md, deg[j]);
+        own += deg[j];
+    }
+    const unsigned maxd = __reduce_max_sync(FULL, md);
     for (unsigned base = 0; base < maxd; base += W) {
         const unsigned k = base + sub;
-        const bool va = k < degA, vb = k < degB;
-        const uint32_t na = va ? __ldg(&C[begA + k]) : 0u;
-        const uint32_t nb = vb ? __ldg(&C[begB + k]) : 0u;
-        fn(va, na, auxA, vb, nb, auxB);
+        uint32_t n[K];
+        bool v[K];
+#pragma unroll
+        for (int j = 0; j < K; j++) {
+            v[j] = k < deg[j];
+            n[j] = v[j] ? __ldg(&C[beg[j] + k]) : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < K; j += 2) fn(j, v[j], n[j], v[j + 1], n[j + 1]);
     }
-    const unsigned own = (sub == 0u) ? degA + degB : 0u;
-    return __reduce_add_sync(FULL, own);
+    return __reduce_add_sync(FULL, sub == 0u ? own : 0u);
 }
 
 // Minimum of x over the CTA folded into *dst with one atomicMin by thread 0

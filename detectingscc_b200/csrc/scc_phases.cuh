@@ -433,30 +433,34 @@ __device__ __forceinline__ void bfs_expand_lanes(Ex &ex, const Graph &g, const W
 }
 
 // Top-down expansion with the virtual-warp schedule (W = 1 << lw lanes per
-// vertex, the reference's fwd_warp/bwd_warp), two frontier vertices per
+// vertex, the reference's fwd_warp/bwd_warp), VWK frontier vertices per
 // lane group in the same steps.
+constexpr int VWK = 4;
 template <class Ex>
-__device__ __forceinline__ void bfs_expand_vw2(Ex &ex, const Graph &g, const Work &w, int dir, uint32_t vA,
-                                               bool actA, uint32_t rA, uint32_t vB, bool actB, uint32_t rB, int lw,
-                                               unsigned par, unsigned nxt)
+__device__ __forceinline__ void bfs_expand_vwk(Ex &ex, const Graph &g, const Work &w, int dir,
+                                               const uint32_t (&v)[VWK], const bool (&act)[VWK],
+                                               const uint32_t (&r)[VWK], int lw, unsigned par, unsigned nxt)
 {
     const uint32_t *R = dir ? g.Br : g.Fr;
     const uint32_t *C = dir ? g.Bc : g.Fc;
-    uint32_t begA = 0, degA = 0, begB = 0, degB = 0;
-    if (actA) { begA = __ldg(&R[vA]); degA = __ldg(&R[vA + 1]) - begA; }
-    if (actB) { begB = __ldg(&R[vB]); degB = __ldg(&R[vB + 1]) - begB; }
     const bool lead = (lane_id() & ((1u << lw) - 1u)) == 0u;
-    const bool hA = degA > HEAVY_T, hB = degB > HEAVY_T;
-    warp_push_chunks(vA, hA && lead ? (degA + CH - 1u) / CH : 0u, w.H[dir][par], &ex.ctl->lc[nxt][C_FH + dir],
-                     w.hcap, ex.ctl);
-    warp_push_chunks(vB, hB && lead ? (degB + CH - 1u) / CH : 0u, w.H[dir][par], &ex.ctl->lc[nxt][C_FH + dir],
-                     w.hcap, ex.ctl);
-    if (hA) degA = 0u;
-    if (hB) degB = 0u;
-    auto fn2 = [&](bool v0, uint32_t n0, uint32_t r0, bool v1, uint32_t n1, uint32_t r1) {
-        bfs_edge_visit2(ex, g, w, dir, v0, n0, r0, v1, n1, r1, par, nxt);
+    uint32_t beg[VWK], deg[VWK];
+#pragma unroll
+    for (int j = 0; j < VWK; j++) {
+        beg[j] = act[j] ? __ldg(&R[v[j]]) : 0u;
+        deg[j] = act[j] ? __ldg(&R[v[j] + 1]) - beg[j] : 0u;
+    }
+#pragma unroll
+    for (int j = 0; j < VWK; j++) {
+        const bool heavy = deg[j] > HEAVY_T;
+        warp_push_chunks(v[j], heavy && lead ? (deg[j] + CH - 1u) / CH : 0u, w.H[dir][par],
+                         &ex.ctl->lc[nxt][C_FH + dir], w.hcap, ex.ctl);
+        if (heavy) deg[j] = 0u;
+    }
+    auto fn = [&](int j, bool v0, uint32_t n0, bool v1, uint32_t n1) {
+        bfs_edge_visit2(ex, g, w, dir, v0, n0, r[j], v1, n1, r[j + 1], par, nxt);
     };
-    count_edges(ex, vw_expand2(begA, degA, rA, begB, degB, rB, (unsigned)lw, C, fn2));
+    count_edges(ex, vw_expandK<VWK>(beg, deg, (unsigned)lw, C, fn));
 }
 
 // One CH-entry chunk of a heavy vertex, expanded by the whole warp.
@@ -681,8 +685,8 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
         const uint32_t nd = (puf || pub) ? (psrc.n + 63u) / 64u : 0u;
         ok = run_pass(ex, (puf || pub) ? PH_BFS_PULL : PH_BFS, [&](unsigned, unsigned nxt) {
             const unsigned par = ex.gl & 1u, cp = par ^ 1u;
-            // virtual-warp items take two groups of frontier vertices
-            const uint32_t isz = (lw < 0) ? gsz : 2u * gsz;
+            // virtual-warp items take VWK groups of frontier vertices
+            const uint32_t isz = (lw < 0) ? gsz : (uint32_t)VWK * gsz;
             const uint32_t ngf = (nf + isz - 1u) / isz, ngb = (nb + isz - 1u) / isz;
             const uint32_t items_f = puf ? 0u : nhf + ngf;
             const uint32_t items_b = pub ? 0u : (bw ? nhb + ngb : 0u);
@@ -715,13 +719,20 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
                         count_verts(ex, valid && lead);
                         bfs_expand_lanes(ex, g, w, dir, v, valid, r, lw, par, nxt);
                     } else {
-                        const uint32_t i2 = i + gsz;
-                        const bool valid2 = i2 < n;
-                        const uint32_t v2 = valid2 ? w.Q[dir][cp][i2] : 0u;
-                        const uint32_t r2 = valid2 ? (w.st[v2] & RMASK) : 0u;
-                        count_verts(ex, valid && lead);
-                        count_verts(ex, valid2 && lead);
-                        bfs_expand_vw2(ex, g, w, dir, v, valid, r, v2, valid2, r2, lw, par, nxt);
+                        uint32_t vk[VWK], rk[VWK];
+                        bool ak[VWK];
+#pragma unroll
+                        for (int j = 0; j < VWK; j++) {
+                            const uint32_t ij = i + (uint32_t)j * gsz;
+                            ak[j] = ij < n;
+                            vk[j] = ak[j] ? w.Q[dir][cp][ij] : 0u;
+                        }
+#pragma unroll
+                        for (int j = 0; j < VWK; j++) {
+                            rk[j] = ak[j] ? (w.st[vk[j]] & RMASK) : 0u;
+                            count_verts(ex, ak[j] && lead);
+                        }
+                        bfs_expand_vwk(ex, g, w, dir, vk, ak, rk, lw, par, nxt);
                     }
                 }
             }
