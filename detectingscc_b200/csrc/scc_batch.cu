@@ -94,14 +94,17 @@ __device__ void batch_one(Ex &ex, const BatchParams &p, uint32_t gi, char *base,
 // The first p.nbig graphs of p.order run one at a time on a whole cluster
 // (when the launch has clusters), the rest one per CTA.  Counters:
 // next[0] for cluster graphs, next[1] for CTA graphs.
-template <int THREADS, bool HONG>
+// CL: the variant with the cluster loop, launched only when the batch has
+// cluster graphs (kept apart so the common one-CTA-per-graph kernel does
+// not carry the cluster path's registers).
+template <int THREADS, bool HONG, bool CL>
 __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_scc_batch(BatchParams p)
 {
     __shared__ uint32_t s_k, s_kb;
     __shared__ Work s_w;   // per-graph carving, kept in shared memory rather than local memory
     bq_init();
     char *mine = p.scratch + (size_t)blockIdx.x * p.scratch_per_cta;
-    if (p.nbig) {
+    if (CL && p.nbig) {
         const unsigned cr = cluster_rank(), cn = cluster_size();
         char *lead = p.scratch + (size_t)((blockIdx.x - cr) / p.lead_div) * p.scratch_per_cta;   // 1-D clusters
         for (;;) {
@@ -127,18 +130,19 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_scc_batch(BatchPara
 }
 
 template <int THREADS>
-void *batch_kernel(bool hong)
+void *batch_kernel(bool hong, bool cl)
 {
-    return hong ? (void *)k_scc_batch<THREADS, true> : (void *)k_scc_batch<THREADS, false>;
+    if (cl) return hong ? (void *)k_scc_batch<THREADS, true, true> : (void *)k_scc_batch<THREADS, false, true>;
+    return hong ? (void *)k_scc_batch<THREADS, true, false> : (void *)k_scc_batch<THREADS, false, false>;
 }
 
-void *pick_batch_kernel(int threads, bool hong)
+void *pick_batch_kernel(int threads, bool hong, bool cl = false)
 {
     switch (threads) {
-    case 128: return batch_kernel<128>(hong);
-    case 256: return batch_kernel<256>(hong);
-    case 512: return batch_kernel<512>(hong);
-    default: return batch_kernel<1024>(hong);
+    case 128: return batch_kernel<128>(hong, cl);
+    case 256: return batch_kernel<256>(hong, cl);
+    case 512: return batch_kernel<512>(hong, cl);
+    default: return batch_kernel<1024>(hong, cl);
     }
 }
 
@@ -151,8 +155,8 @@ size_t sccb_batch_smem(int threads, uint32_t qcap) { return batch_smem(threads, 
 int sccb_batch_ctas(int threads, uint32_t qcap, int nsm, uint32_t *out, int cluster)
 {
     const size_t smem = batch_smem(threads, qcap);
-    for (int h = 0; h < 2; h++) {
-        void *fn = pick_batch_kernel(threads, h != 0);
+    for (int h = 0; h < 4; h++) {
+        void *fn = pick_batch_kernel(threads, (h & 1) != 0, h >= 2);
         if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
             (cluster > 8 && cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)) {
             cudaGetLastError();
@@ -182,7 +186,7 @@ int sccb_batch_ctas(int threads, uint32_t qcap, int nsm, uint32_t *out, int clus
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     int ncl = 0;
-    if (cudaOccupancyMaxActiveClusters(&ncl, pick_batch_kernel(threads, true), &cfg) != cudaSuccess || ncl <= 0) {
+    if (cudaOccupancyMaxActiveClusters(&ncl, pick_batch_kernel(threads, true, true), &cfg) != cudaSuccess || ncl <= 0) {
         cudaGetLastError();
         return SCC_ERR_CUDA;
     }
@@ -195,7 +199,7 @@ int sccb_batch_launch(const BatchParams &p, int threads, bool hong, uint32_t nct
     BatchParams q = p;
     void *args[] = {&q};
     cudaError_t e;
-    if (cluster <= 1) {
+    if (cluster <= 1 || p.nbig == 0) {   // no cluster graphs: the one-CTA-per-graph kernel
         e = cudaLaunchKernel(pick_batch_kernel(threads, hong), dim3(ncta), dim3(threads), args,
                              batch_smem(threads, p.qcap), st);
     } else {
@@ -211,7 +215,7 @@ int sccb_batch_launch(const BatchParams &p, int threads, bool hong, uint32_t nct
         cfg.stream = st;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        e = cudaLaunchKernelExC(&cfg, pick_batch_kernel(threads, hong), args);
+        e = cudaLaunchKernelExC(&cfg, pick_batch_kernel(threads, hong, true), args);
     }
     if (e != cudaSuccess) {
         cudaGetLastError();
