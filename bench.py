@@ -15,8 +15,10 @@ driver, labels canonicalised and written).
           L2 flushed (256 MiB write) before every step, CUDA events on the
           launching stream, max over ranks.
   e2e   : the same call through the C ABI with HOST (pinned) CSR buffers:
-          the H2D copy of the CSR and the D2H copy of the labels are inside
-          the timed region.
+          the H2D copy of the forward CSR (the reverse one is built on the
+          device, SCC_FLAG_DERIVE_REVERSE) and the D2H copy of the labels are
+          inside the timed region; e2e.both_csr_copied times the call that
+          copies both CSRs.
 With --gpus N > 1 (torchrun) every rank runs an independent replica of the
 graph (the plain path does not shard); value = N * E / max-over-ranks time.
 
@@ -228,19 +230,29 @@ def run_ours(args):
     t_step = _max_over_ranks(sum(step_ms) / len(step_ms), world)
     t_kern = _max_over_ranks(sum(kern_ms) / len(kern_ms), world)
 
-    # end-to-end: host pinned CSR in, labels out, through the C ABI
+    # end-to-end: host pinned CSR in, labels out, through the C ABI; twice:
+    # both CSRs copied (the reference's interface), and only the forward CSR
+    # copied with the reverse one built on the device (SCC_FLAG_DERIVE_REVERSE)
     hlab_np = hlab.numpy().view(np.uint32)
-    for _ in range(max(1, args.warmup)):
-        eng.run(hg, algo=cfg["algo"], t1=cfg["t1"], t2=cfg["t2"], warp=cfg["warp"], out=hlab_np)
-    _barrier(world)
-    e2e_ms = []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        r = eng.run(hg, algo=cfg["algo"], t1=cfg["t1"], t2=cfg["t2"], warp=cfg["warp"], out=hlab_np)
-        e2e_ms.append((time.perf_counter() - t0) * 1e3)
-    _barrier(world)
-    t_e2e = _max_over_ranks(sum(e2e_ms) / len(e2e_ms), world)
-    assert r.num_sccs == res.num_sccs
+
+    def e2e_leg(derive):
+        for _ in range(max(1, args.warmup)):
+            eng.run(hg, algo=cfg["algo"], t1=cfg["t1"], t2=cfg["t2"], warp=cfg["warp"], out=hlab_np,
+                    derive_reverse=derive)
+        _barrier(world)
+        ms = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            r = eng.run(hg, algo=cfg["algo"], t1=cfg["t1"], t2=cfg["t2"], warp=cfg["warp"], out=hlab_np,
+                        derive_reverse=derive)
+            ms.append((time.perf_counter() - t0) * 1e3)
+        _barrier(world)
+        assert r.num_sccs == res.num_sccs
+        return _max_over_ranks(sum(ms) / len(ms), world), r.labels.copy()
+
+    t_e2e_both, lab_both = e2e_leg(False)
+    t_e2e, lab_fwd = e2e_leg(True)
+    assert np.array_equal(lab_both, lab_fwd)
 
     B_alg = 8 * ins["edges_scanned"] + 12 * ins["vertex_visits"]
     peak, peak_kind = _peak_hbm()
@@ -277,8 +289,13 @@ def run_ours(args):
                      "kernel": "k_scc_grid (persistent cooperative SCC kernel)"},
         "e2e": {"value": round(world * E / (t_e2e * 1e-3) / 1e6, 2), "unit": "Medges/s",
                 "ms_per_step": round(t_e2e, 3),
-                "h2d_bytes_per_step": int(4 * (2 * (V + 2) + 2 * E)),
-                "d2h_bytes_per_step": int(4 * V + 512)},
+                "h2d_bytes_per_step": int(4 * ((V + 2) + E)),
+                "d2h_bytes_per_step": int(4 * V + 512),
+                "path": "forward CSR from pinned host memory, reverse CSR built on the device "
+                        "(SCC_FLAG_DERIVE_REVERSE), labels back to pinned host memory",
+                "both_csr_copied": {"value": round(world * E / (t_e2e_both * 1e-3) / 1e6, 2),
+                                    "ms_per_step": round(t_e2e_both, 3),
+                                    "h2d_bytes_per_step": int(4 * (2 * (V + 2) + 2 * E))}},
         "gpu_launches": int(launches),
         "clocks": clk,
     }

@@ -74,12 +74,13 @@ FLAG_DEVICE = 0x4
 FLAG_INSTRUMENT = 0x8
 FLAG_FORCE_GRID = 0x10
 FLAG_FORCE_BLOCK = 0x20
+FLAG_DERIVE_REVERSE = 0x80
 FLAG_BATCH_SEQUENTIAL = 0x40
 MAX_VERTICES = 268435454
 
 # every symbol include/scc_b200.h and include/scc_compat.h declare
 C_SYMBOLS = ["scc_create", "scc_destroy", "scc_run", "scc_set_tuning", "scc_status_string",
-             "scc_version", "scc_get_trace", "scc_load_graph", "scc_save_binary", "scc_graph_from_arcs",
+             "scc_version", "scc_get_trace", "scc_derive_reverse", "scc_load_graph", "scc_save_binary", "scc_graph_from_arcs",
              "scc_free_host_graph", "scc_reference_call", "scc_batch_create", "scc_batch_run",
              "scc_batch_destroy", "scc_run_noalloc", "scc_batch_set_schedule", "scc_batch_get_schedule",
              "scc_batch_autotune", "scc_batch_info", "scc_batch_set_cluster", "scc_batch_get_cluster", "scc_server_create", "scc_server_submit",
@@ -145,6 +146,7 @@ def lib():
     L.scc_server_info.argtypes = [vp, ctypes.POINTER(u64), ctypes.POINTER(u64), ctypes.POINTER(u64), ctypes.POINTER(u64)]
     L.scc_server_launches.argtypes = [vp, ctypes.POINTER(u64)]
     L.scc_server_destroy.argtypes = [vp]
+    L.scc_derive_reverse.argtypes = [vp, vp, vp, u32, u32, vp, vp, vp]
     L.scc_get_trace.argtypes = [vp, ctypes.POINTER(u64), u32, ctypes.POINTER(u32), ctypes.POINTER(u64)]
     _lib = L
     return L

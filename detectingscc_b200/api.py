@@ -121,13 +121,17 @@ class Engine:
         return out
 
     def run(self, g: Graph, algo="h", t1=True, t2=True, warp=1, labels=True,
-            instrument=False, force=None, out: Optional[np.ndarray] = None) -> Result:
+            instrument=False, force=None, out: Optional[np.ndarray] = None,
+            derive_reverse: bool = False) -> Result:
         """Run on a host graph: the call copies the CSR in and the labels out.
 
         out: optional preallocated host array (e.g. pinned) of V uint32.
+        derive_reverse: copy only the forward CSR and build the reverse one on
+        the device (g.Br / g.Bc are not read).
         """
         flags = (N.FLAG_TRIM1 if t1 else 0) | (N.FLAG_TRIM2 if t2 else 0)
         flags |= N.FLAG_INSTRUMENT if instrument else 0
+        flags |= N.FLAG_DERIVE_REVERSE if derive_reverse else 0
         if force == "grid":
             flags |= N.FLAG_FORCE_GRID
         elif force == "block":
@@ -144,8 +148,16 @@ class Engine:
         return Result(out[:g.V] if labels else None, st.num_sccs, st.num_trim1, st.num_trim2,
                       st.num_pivot, st.as_dict())
 
+    def derive_reverse(self, V: int, E: int, Fr, Fc, Br, Bc, stream=None) -> None:
+        """Fill device arrays Br (V+2) and Bc (E) with the reverse CSR of (Fr, Fc)."""
+        if stream is None and hasattr(Fr, "device") and getattr(Fr.device, "type", "") == "cuda":
+            import torch
+            stream = torch.cuda.current_stream(Fr.device).cuda_stream
+        N.check(self._lib.scc_derive_reverse(self._h, _ptr(Fr), _ptr(Fc), int(V), int(E), _ptr(Br), _ptr(Bc), stream),
+                "scc_derive_reverse")
+
     def run_device(self, V: int, E: int, Fr, Fc, Br, Bc, labels_out=None, algo="h", t1=True, t2=True,
-                   warp=1, instrument=False, stream=None, force=None) -> Result:
+                   warp=1, instrument=False, stream=None, force=None, derive_reverse: bool = False) -> Result:
         """Run on device-resident CSR (torch CUDA tensors or raw device pointers).
 
         labels_out: device buffer of V uint32/int32 entries, or None.
@@ -154,6 +166,7 @@ class Engine:
         """
         flags = N.FLAG_DEVICE | (N.FLAG_TRIM1 if t1 else 0) | (N.FLAG_TRIM2 if t2 else 0)
         flags |= N.FLAG_INSTRUMENT if instrument else 0
+        flags |= N.FLAG_DERIVE_REVERSE if derive_reverse else 0
         if force == "grid":
             flags |= N.FLAG_FORCE_GRID
         elif force == "block":

@@ -301,6 +301,7 @@ extern "C" int scc_destroy(scc_context *ctx)
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     cudaFree(ctx->ws);
     cudaFree(ctx->dFr); cudaFree(ctx->dFc); cudaFree(ctx->dBr); cudaFree(ctx->dBc); cudaFree(ctx->dlab);
+    cudaFree(ctx->tsrc); cudaFree(ctx->tkey); cudaFree(ctx->ttmp); cudaFree(ctx->tctl);
     if (ctx->hctl) cudaFreeHost(ctx->hctl);
     cudaFree(ctx->dtrace);
     if (ctx->htrace) cudaFreeHost(ctx->htrace);
@@ -361,7 +362,8 @@ extern "C" int scc_run(scc_context *ctx, const scc_csr_view *gv, int algo, uint3
     const uint32_t V = gv->num_vertices, E = gv->num_edges;
     if (V > SCC_MAX_VERTICES || E > SCC_MAX_EDGES) return SCC_ERR_TOO_LARGE;
     if (V == 0) return SCC_OK;
-    if (!gv->Fr || !gv->Br || (E && (!gv->Fc || !gv->Bc))) return SCC_ERR_INVALID_ARG;
+    const bool derive = (flags & SCC_FLAG_DERIVE_REVERSE) != 0;
+    if (!gv->Fr || (!derive && !gv->Br) || (E && (!gv->Fc || (!derive && !gv->Bc)))) return SCC_ERR_INVALID_ARG;
     const bool dev = (flags & SCC_FLAG_DEVICE) != 0;
     const bool instr = (flags & SCC_FLAG_INSTRUMENT) != 0;
     std::lock_guard<std::mutex> lock(ctx->mu);
@@ -376,17 +378,21 @@ extern "C" int scc_run(scc_context *ctx, const scc_csr_view *gv, int algo, uint3
     CK(cudaEventRecord(ctx->ev[0], st));
     Graph g{V, E, gv->Fr, gv->Fc, gv->Br, gv->Bc, 0u};
     uint32_t *dout = labels_out;
-    if (!dev) {
+    if (!dev || derive) {
         rc = ensure_csr_mirror(ctx, V, E);
         if (rc != SCC_OK) return rc;
+    }
+    if (!dev) {
         CK(cudaMemcpyAsync(ctx->dFr, gv->Fr, ((size_t)V + 2) * 4, cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(ctx->dBr, gv->Br, ((size_t)V + 2) * 4, cudaMemcpyHostToDevice, st));
+        if (!derive) CK(cudaMemcpyAsync(ctx->dBr, gv->Br, ((size_t)V + 2) * 4, cudaMemcpyHostToDevice, st));
         if (E) {
             CK(cudaMemcpyAsync(ctx->dFc, gv->Fc, (size_t)E * 4, cudaMemcpyHostToDevice, st));
-            CK(cudaMemcpyAsync(ctx->dBc, gv->Bc, (size_t)E * 4, cudaMemcpyHostToDevice, st));
+            if (!derive) CK(cudaMemcpyAsync(ctx->dBc, gv->Bc, (size_t)E * 4, cudaMemcpyHostToDevice, st));
         }
         g.Fr = ctx->dFr; g.Fc = ctx->dFc; g.Br = ctx->dBr; g.Bc = ctx->dBc;
         dout = labels_out ? ctx->dlab : nullptr;
+    } else if (derive) {
+        g.Br = ctx->dBr; g.Bc = ctx->dBc;   // built below from the caller's forward CSR
     }
     if (!E) { g.Fc = g.Fc ? g.Fc : ctx->work.st; g.Bc = g.Bc ? g.Bc : ctx->work.st; }
     g.vec = ((((uintptr_t)g.Fr) | ((uintptr_t)g.Br)) & 15u) == 0u ? 1u : 0u;
@@ -397,6 +403,12 @@ extern "C" int scc_run(scc_context *ctx, const scc_csr_view *gv, int algo, uint3
     ctx->hctl->trace = ctx->dtrace;
     ctx->hctl->trace_cap = ctx->dtrace ? ctx->trace_cap : 0u;
     CK(cudaMemcpyAsync(ctx->work.ctl, ctx->hctl, sizeof(Ctl), cudaMemcpyHostToDevice, st));
+    if (derive) {
+        // after the control block is zeroed: input errors found here stop the SCC kernel at its entry
+        rc = sccb_derive_reverse(ctx, g.Fr, g.Fc, V, E, const_cast<uint32_t *>(g.Br), const_cast<uint32_t *>(g.Bc),
+                                 ctx->work.ctl, st);
+        if (rc != SCC_OK) return rc;
+    }
     CK(cudaMemsetAsync(ctx->work.pivkey, 0, hong ? (4 * ((size_t)V + 1) + 8) * 8 : 8, st));
 
 

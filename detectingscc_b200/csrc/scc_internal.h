@@ -25,6 +25,13 @@ struct scc_context {
     uint32_t *dFr = nullptr, *dFc = nullptr, *dBr = nullptr, *dBc = nullptr, *dlab = nullptr;
     size_t capV = 0, capE = 0;
 
+    // reverse CSR built on the device (SCC_FLAG_DERIVE_REVERSE): edge sources,
+    // sorted targets and the sort's temporary storage
+    uint32_t *tsrc = nullptr, *tkey = nullptr;
+    void *ttmp = nullptr;
+    sccb::Ctl *tctl = nullptr;          // error word of scc_derive_reverse
+    size_t tcapE = 0, ttmp_bytes = 0;
+
     // tuning
     uint32_t tail_vertices = 1024;       // CTA 0 finishes alone at or below this live count
     uint32_t block_max_vertices = 16384; // graphs up to this size run on one CTA
@@ -49,5 +56,9 @@ struct scc_context {
 };
 
 int scc_ctx_reserve(scc_context *ctx, uint32_t V, uint32_t E);
+// Builds Br and Bc (device) from Fr and Fc (device) on stream st; errors in
+// the input are raised in ctx->work.ctl.  Allocates its temporaries in ctx.
+int sccb_derive_reverse(scc_context *ctx, const uint32_t *dFr, const uint32_t *dFc, uint32_t V, uint32_t E,
+                        uint32_t *dBr, uint32_t *dBc, sccb::Ctl *ctl, cudaStream_t st);
 // Bytes of the workspace scc_ctx_reserve allocates for a graph.
 size_t scc_ctx_ws_need(uint32_t V, uint32_t E);

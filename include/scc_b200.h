@@ -52,6 +52,10 @@ typedef enum {
 #define SCC_FLAG_FORCE_GRID 0x10u    /* always use the whole-GPU persistent launch */
 #define SCC_FLAG_FORCE_BLOCK 0x20u   /* always use the single-CTA launch */
 #define SCC_FLAG_BATCH_SEQUENTIAL 0x40u /* scc_batch_run: one plain scc_run per graph (the baseline) */
+#define SCC_FLAG_DERIVE_REVERSE 0x80u /* scc_run: Br/Bc are not read (may be NULL); the reverse CSR is built on
+                                         the device from Fr/Fc, in the reference loader's layout (in-lists in
+                                         ascending source order), so only the forward CSR crosses PCIe.  No
+                                         counterpart in the reference, whose loader builds both on the host. */
 
 #define SCC_MAX_VERTICES 268435454u  /* 2^28 - 2 */
 #define SCC_MAX_EDGES 4294967040u     /* 2^32 - 256 */
@@ -108,6 +112,15 @@ int scc_destroy(scc_context *ctx);
  * print their count. */
 int scc_run(scc_context *ctx, const scc_csr_view *g, int algo, uint32_t flags, int warp_width,
             uint32_t *labels_out, scc_stats *stats, void *stream);
+
+/* The reverse CSR built on the device from the forward one, in the reference
+ * loader's layout (load.cpp:47-113: Br[0] = Br[1] = 0, in-lists in ascending
+ * source order).  All pointers are device pointers; Br has V+2 entries, Bc E.
+ * Synchronous on `stream`.  Ids outside [1, V] or malformed offsets give
+ * SCC_ERR_BAD_GRAPH.  No counterpart in the reference, which builds both
+ * CSRs on the host.  Uses (and keeps) temporaries of about 12 B per edge. */
+int scc_derive_reverse(scc_context *ctx, const uint32_t *Fr, const uint32_t *Fc, uint32_t V, uint32_t E,
+                       uint32_t *Br, uint32_t *Bc, void *stream);
 
 /* Tuning knobs (used by tests and the batch autotuner):
  *   "tail_vertices"       live-vertex count under which CTA 0 finishes alone
