@@ -43,9 +43,10 @@ template <bool HONG, class Ex>
 __device__ void batch_one(Ex &ex, const BatchParams &p, uint32_t gi, char *base, Work &s_w)
 {
     const BatchGraph bg = p.graphs[gi];
+    const unsigned long long t0 = gtimer();
     if (bg.V == 0u) {
         if (ex.leader()) {
-            p.res[gi] = BatchRes{0ull, 0ull, 0ull, 0, 0};
+            p.res[gi] = BatchRes{0ull, 0ull, 0ull, 0, 0, 0ull};
             if (p.done) {
                 __threadfence_system();
                 *(volatile unsigned *)&p.done[gi] = 1u;
@@ -85,7 +86,8 @@ __device__ void batch_one(Ex &ex, const BatchParams &p, uint32_t gi, char *base,
             o[v - 1u] = l <= bg.V ? w.smin[l] : 0u;
         }
     }
-    if (ex.leader()) p.res[gi] = BatchRes{w.ctl->n_trim1, w.ctl->n_trim2, w.ctl->n_pivot, err, w.ctl->where};
+    if (ex.leader())
+        p.res[gi] = BatchRes{w.ctl->n_trim1, w.ctl->n_trim2, w.ctl->n_pivot, err, w.ctl->where, gtimer() - t0};
     if (p.done) __threadfence_system();   // labels and result reach the host before the flag
     ex.sync();   // the slice is reused by the next graph
     if (p.done && ex.leader()) *(volatile unsigned *)&p.done[gi] = 1u;
@@ -238,14 +240,16 @@ uint32_t sccb_launch_ctas(uint32_t resident, uint32_t n, uint32_t nbig, int clus
 
 // Processing order: graphs with at least big_vertices vertices first (they
 // run on whole clusters), then the rest, each part largest first.
-uint32_t sccb_order(const BatchGraph *g, uint32_t n, uint32_t big_vertices, int cluster, uint32_t *order)
+uint32_t sccb_order(const BatchGraph *g, uint32_t n, uint32_t big_vertices, int cluster, uint32_t *order,
+                    const unsigned long long *cost)
 {
     const bool use = cluster > 1;
     std::iota(order, order + n, 0u);
     auto big = [&](uint32_t i) { return use && g[i].V >= big_vertices; };
+    auto w = [&](uint32_t i) { return cost ? cost[i] : (unsigned long long)g[i].E + g[i].V; };
     std::stable_sort(order, order + n, [&](uint32_t a, uint32_t c) {
         if (big(a) != big(c)) return big(a);
-        return (unsigned long long)g[a].E + g[a].V > (unsigned long long)g[c].E + g[c].V;
+        return w(a) > w(c);
     });
     uint32_t nb = 0;
     while (nb < n && big(order[nb])) nb++;
@@ -273,6 +277,9 @@ struct scc_batch {
     int cluster = 1;                 // CTAs per cluster (1: every graph on one CTA)
     uint32_t big_vertices = 16384;   // graphs with at least this many vertices run on a whole cluster
     uint32_t nbig = 0;
+    // per-graph times of the last batched run, and whether the order follows them
+    std::vector<unsigned long long> last_ns;
+    bool by_cost = false;
     // captured launch
     cudaGraphExec_t gexec = nullptr;
     int g_algo = 0, g_w = 0, g_threads = 0, g_cluster = 0, g_check = 0;
@@ -295,7 +302,9 @@ static void batch_free(scc_batch *b)
 static int batch_upload_order(scc_batch *b, int cluster, uint32_t big_vertices)
 {
     std::vector<uint32_t> order(std::max<uint32_t>(b->n, 1u));
-    const uint32_t nb = sccb_order(b->hgraphs.data(), b->n, big_vertices, cluster, order.data());
+    const bool cost = b->by_cost && b->last_ns.size() == b->n;
+    const uint32_t nb = sccb_order(b->hgraphs.data(), b->n, big_vertices, cluster, order.data(),
+                                   cost ? b->last_ns.data() : nullptr);
     if (b->n && (cudaMemcpyAsync(b->dorder, order.data(), (size_t)b->n * 4, cudaMemcpyHostToDevice, b->stream) != cudaSuccess ||
                  cudaStreamSynchronize(b->stream) != cudaSuccess)) {
         cudaGetLastError();
@@ -477,7 +486,8 @@ static int batch_run_sequential(scc_batch *b, int algo, uint32_t flags, int w, s
         scc_stats st;
         int rc = scc_run(b->ctx, &v, algo, (flags & ~SCC_FLAG_BATCH_SEQUENTIAL) | SCC_FLAG_DEVICE, w,
                          b->dout + bg.off_out, &st, b->stream);
-        b->hres[i] = BatchRes{st.num_trim1, st.num_trim2, st.num_pivot, rc, st.error_where};
+        b->hres[i] = BatchRes{st.num_trim1, st.num_trim2, st.num_pivot, rc, st.error_where,
+                              (unsigned long long)(st.total_ms * 1e6)};
         if (stats) stats->gpu_launches += st.gpu_launches;
     }
     cudaEventRecord(b->ev[1], b->stream);
@@ -544,6 +554,10 @@ extern "C" int scc_batch_run(scc_batch *b, int algo, uint32_t flags, int warp_wi
     if (cudaStreamSynchronize(b->stream) != cudaSuccess) { cudaGetLastError(); return SCC_ERR_CUDA; }
     int first_err = SCC_OK;
     unsigned long long tot = 0;
+    if (!(flags & SCC_FLAG_BATCH_SEQUENTIAL)) {
+        b->last_ns.resize(b->n);
+        for (uint32_t i = 0; i < b->n; i++) b->last_ns[i] = b->hres[i].ns;
+    }
     for (uint32_t i = 0; i < b->n; i++) {
         const BatchRes &r = b->hres[i];
         if (results) results[i] = scc_batch_result{r.trim1 + r.trim2 + r.pivot, r.trim1, r.status, 0u};
@@ -611,6 +625,27 @@ extern "C" int scc_batch_autotune(scc_batch *b, int algo, uint32_t flags, int wa
         }
     }
     rc = scc_batch_set_cluster(b, bc, bb);
+    if (rc != SCC_OK) return rc;
+    // profile-guided order: longest-processing-time first by the graphs' own
+    // times in a run with the chosen schedule (size is a poor proxy: a chain
+    // of many small SCCs takes far longer than a random graph of its size)
+    {
+        float ms = 0.f;
+        rc = time_it(&ms);   // leaves the per-graph times of its last run in last_ns
+        if (rc != SCC_OK) return rc;
+        b->by_cost = true;
+        rc = batch_upload_order(b, b->cluster, b->big_vertices);
+        if (rc != SCC_OK) return rc;
+        float ms2 = 0.f;
+        rc = time_it(&ms2);
+        if (rc != SCC_OK) return rc;
+        if (ms2 < best) {
+            best = ms2;
+        } else {
+            b->by_cost = false;
+            rc = batch_upload_order(b, b->cluster, b->big_vertices);
+        }
+    }
     if (best_threads) *best_threads = bt;
     if (best_qcap) *best_qcap = bq;
     if (best_ms) *best_ms = best / 2.f;

@@ -15,6 +15,7 @@ struct BatchGraph {
 struct BatchRes {
     unsigned long long trim1, trim2, pivot;
     int status, where;
+    unsigned long long ns;      // time the graph took on its CTA or cluster (%globaltimer)
 };
 
 struct BatchParams {
@@ -49,5 +50,7 @@ int sccb_batch_ctas(int threads, uint32_t qcap, int nsm, uint32_t *out, int clus
 int sccb_batch_launch(const BatchParams &p, int threads, bool hong, uint32_t ncta, cudaStream_t st, int cluster = 1);
 // CTAs of a launch: at most `resident`, a whole number of clusters.
 uint32_t sccb_launch_ctas(uint32_t resident, uint32_t n, uint32_t nbig, int cluster);
-// Processing order (cluster graphs first, each part largest first); returns nbig.
-uint32_t sccb_order(const BatchGraph *g, uint32_t n, uint32_t big_vertices, int cluster, uint32_t *order);
+// Processing order (cluster graphs first, each part longest first: by cost[i]
+// when given, measured times of an earlier run, else by V + E); returns nbig.
+uint32_t sccb_order(const BatchGraph *g, uint32_t n, uint32_t big_vertices, int cluster, uint32_t *order,
+                    const unsigned long long *cost = nullptr);

@@ -41,7 +41,7 @@ constexpr int E_NOT_CONVERGED = 21;
 constexpr int E_TIMEOUT = 22;
 constexpr int E_BAD_GRAPH = 23;
 
-enum { C_FQ = 0, C_BQ = 1, C_FH = 2, C_BH = 3, C_LIST = 4, C_FE = 5, C_BE = 6, NCNT = 8 };
+enum { C_FQ = 0, C_BQ = 1, C_FH = 2, C_BH = 3, C_LIST = 4, C_FE = 5, C_BE = 6, C_RNG = 7, NCNT = 8 };
 
 struct __align__(128) Ctl {
     // grid barrier arrival counter and the sticky error code share one
@@ -717,17 +717,21 @@ __device__ __forceinline__ uint32_t split_name(uint32_t V, uint32_t p, uint32_t 
 
 // Per-range atomicMax of pivot keys with warp aggregation over lanes that
 // share a range (match.any + redux) and a read before the atomic.
-__device__ __forceinline__ void range_max_atomic(bool valid, uint32_t r, unsigned long long key,
+// Returns true in exactly one lane of the whole launch per range: the one
+// whose atomicMax found the slot still empty (the range's first bid).
+__device__ __forceinline__ bool range_max_atomic(bool valid, uint32_t r, unsigned long long key,
                                                  unsigned long long *pivkey)
 {
     unsigned grp = __match_any_sync(FULL, valid ? r : 0xFFFFFFFFu);
     unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
     unsigned mhi = __reduce_max_sync(grp, hi);
     unsigned mlo = __reduce_max_sync(grp, hi == mhi ? lo : 0u);
+    bool first = false;
     if (valid && lane_id() == (unsigned)(__ffs(grp) - 1)) {
         unsigned long long k = ((unsigned long long)mhi << 32) | mlo;
-        if (k > *(volatile unsigned long long *)&pivkey[r]) atomicMax(&pivkey[r], k);
+        if (k > *(volatile unsigned long long *)&pivkey[r]) first = atomicMax(&pivkey[r], k) == 0ull;
     }
+    return first;
 }
 
 }  // namespace sccb

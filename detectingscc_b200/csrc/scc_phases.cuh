@@ -592,19 +592,21 @@ __device__ __forceinline__ void bfs_pull2(Ex &ex, const Graph &g, const Work &w,
 }
 
 // Seed predicates for the first BFS pass.
+// A seed takes list entry x: operator() says whether it seeds, vert() which
+// vertex it seeds.
 struct SeedOne {      // the single first pivot
     uint32_t p;
     __device__ __forceinline__ bool operator()(const Work &, uint32_t v) const { return v == p; }
-};
-struct SeedPivkey {   // per-range pivots (selectPivots, scc_kernels.cu:4-19)
-    __device__ __forceinline__ bool operator()(const Work &w, uint32_t v) const
-    {
-        uint32_t s = w.st[v];
-        return s != DEAD && key_vertex(w.pivkey[s & RMASK]) == v;
-    }
+    __device__ __forceinline__ uint32_t vert(const Work &, uint32_t x) const { return x; }
 };
 struct SeedRoot {     // colouring roots (selectPivotColoring, scc_kernels.cu:567-580)
     __device__ __forceinline__ bool operator()(const Work &w, uint32_t v) const { return w.st[v] == v; }
+    __device__ __forceinline__ uint32_t vert(const Work &, uint32_t x) const { return x; }
+};
+struct SeedRanges {   // per-range pivots (selectPivots, scc_kernels.cu:4-19), walked over the
+                      // list of live ranges instead of every live vertex
+    __device__ __forceinline__ bool operator()(const Work &w, uint32_t r) const { return w.pivkey[r] != 0ull; }
+    __device__ __forceinline__ uint32_t vert(const Work &w, uint32_t r) const { return key_vertex(w.pivkey[r]); }
 };
 
 // Forward (and backward) reachability to closure.  Pass 0 walks src, tests
@@ -653,8 +655,9 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
             unsigned slot = (lw < 0) ? lane_id() : (lane_id() >> lw);
             uint32_t i = it * gsz + slot;
             bool valid = i < src.n;
-            uint32_t v = valid ? src.at(i) : 0u;
-            bool act = valid && seed(w, v);
+            const uint32_t x = valid ? src.at(i) : 0u;
+            bool act = valid && seed(w, x);
+            uint32_t v = act ? seed.vert(w, x) : x;
             bool lead = (lw <= 0) || ((lane_id() & ((1u << lw) - 1u)) == 0u);
             uint32_t r = 0;
             if (act && lead) r = atomicOr(&w.st[v], bits) & RMASK;
@@ -854,7 +857,11 @@ __device__ bool ph_hong_update(Ex &ex, const Graph &g, const Work &w, VList src,
                 if (single) mn = scc ? min(mn, v[j]) : mn;
                 else smin_fold(scc, p, v[j], w.smin);
                 bq_push(0, surv, v[j], w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 15);
-                if (fold) range_max_atomic(surv, nr, surv ? pivot_key(g, v[j]) : 0ull, w.pivkey);
+                if (fold) {
+                    // the new ranges are listed by their first bid (as in ph_pivots)
+                    const bool first = range_max_atomic(surv, nr, surv ? pivot_key(g, v[j]) : 0ull, w.pivkey);
+                    warp_push(first, nr, w.Q[0][ex.gl & 1u], &ex.ctl->lc[nxt][C_RNG], g.V + 1u, ex.ctl, 22);
+                }
             }
             count_verts_n(ex, (unsigned)ok[0] + ok[1] + ok[2] + ok[3]);
         }
@@ -954,13 +961,17 @@ __device__ bool ph_compact_rename(Ex &ex, const Graph &g, const Work &w, VList s
 template <class Ex>
 __device__ bool ph_pivots(Ex &ex, const Graph &g, const Work &w, VList src)
 {
-    return run_pass(ex, PH_PIVOTS, [&](unsigned, unsigned) {
+    // every range is listed once, by its first bid, in Q[0][parity of this
+    // pass]: the next pass seeds the pivots from that list
+    return run_pass(ex, PH_PIVOTS, [&](unsigned, unsigned nxt) {
+        const unsigned par = ex.gl & 1u;
         for (uint32_t base = ex.wid() * 32u; base < src.n; base += ex.nwarps() * 32u) {
             uint32_t i = base + lane_id();
             bool valid = i < src.n;
             uint32_t v = valid ? src.at(i) : 0u;
             uint32_t r = valid ? (w.st[v] & RMASK) : 0u;
-            range_max_atomic(valid, r, valid ? pivot_key(g, v) : 0ull, w.pivkey);
+            const bool first = range_max_atomic(valid, r, valid ? pivot_key(g, v) : 0ull, w.pivkey);
+            warp_push(first, r, w.Q[0][par], &ex.ctl->lc[nxt][C_RNG], g.V + 1u, ex.ctl, 21);
         }
     });
 }
@@ -972,6 +983,7 @@ struct Carry {
     unsigned gl;
     unsigned lsel;
     uint32_t nL;
+    uint32_t nR;    // Hong: ranges listed by the last bidding pass (in Q[0][its parity])
 };
 
 enum { RUN_DONE = 0, RUN_SWITCH = 1, RUN_ERROR = -1 };
@@ -986,9 +998,11 @@ __device__ int hong_loop(Ex &ex, const Graph &g, const Work &w, Carry &cy, uint3
         if (Ex::grid && cy.nL <= tail_n) { cy.gl = ex.gl; return RUN_SWITCH; }
         if (ex.leader()) ex.ctl->outer++;
         const VList L{w.L[cy.lsel], cy.nL, 0u};
-        if (!ph_bfs(ex, g, w, L, SeedPivkey{}, true, -1, L)) return RUN_ERROR;
+        const VList R{w.Q[0][(ex.gl & 1u) ^ 1u], cy.nR, 0u};   // written by the previous pass
+        if (!ph_bfs(ex, g, w, R, SeedRanges{}, true, -1, L)) return RUN_ERROR;
         if (!ph_hong_update(ex, g, w, L, w.L[cy.lsel ^ 1u], false, true)) return RUN_ERROR;
         cy.nL = last_count(ex, C_LIST);
+        cy.nR = last_count(ex, C_RNG);
         cy.lsel ^= 1u;
         cy.gl = ex.gl;
     }
@@ -1070,6 +1084,7 @@ __device__ int hong_front(Ex &ex, const Graph &g, const Work &w, bool t1, bool t
     const VList L{w.L[0], cy.nL, 0u};
     if (!ph_propagate<false>(ex, g, w, L)) return RUN_ERROR;
     if (!ph_pivots(ex, g, w, L)) return RUN_ERROR;
+    cy.nR = last_count(ex, C_RNG);
     cy.gl = ex.gl;
     return RUN_DONE;
 }

@@ -291,7 +291,9 @@ int scc_batch_get_schedule(scc_batch *b, int *threads, uint32_t *qcap);
 int scc_batch_set_cluster(scc_batch *b, int cluster, uint32_t big_vertices);
 int scc_batch_get_cluster(scc_batch *b, int *cluster, uint32_t *big_vertices, uint32_t *num_cluster_graphs);
 /* Times every candidate schedule on the batch and keeps the fastest: CTA
- * size and staging slice first, then cluster size and big_vertices. */
+ * size and staging slice first, then cluster size and big_vertices, then
+ * the processing order (largest first by size, or longest first by each
+ * graph's own time in a run with the chosen schedule). */
 int scc_batch_autotune(scc_batch *b, int algo, uint32_t flags, int warp_width, int *best_threads,
                        uint32_t *best_qcap, float *best_ms);
 int scc_batch_info(scc_batch *b, uint64_t *num_vertices, uint64_t *num_edges, uint32_t *num_graphs);
