@@ -799,6 +799,15 @@ __device__ bool ph_propagate(Ex &ex, const Graph &g, const Work &w, VList src0)
                     bool valid = i < src.n;
                     uint32_t v = valid ? src.at(i) : 0u;
                     uint32_t c = valid ? (w.st[v] & RMASK) : 0u;
+                    if (!MAXP && valid && c != v) {
+                        // pointer jumping: the name of v's name is also reachable from v
+                        // (the same fixpoint, reached in fewer sweeps on long chains)
+                        const uint32_t s2 = w.st[c];
+                        if (s2 != DEAD && (s2 & RMASK) < c) {
+                            c = s2 & RMASK;
+                            atomicMin(&w.st[v], c);
+                        }
+                    }
                     uint32_t beg = 0, deg = 0;
                     if (valid) { beg = __ldg(&g.Br[v]); deg = __ldg(&g.Br[v + 1]) - beg; }
                     bool heavy = deg > HEAVY_T;
