@@ -469,6 +469,7 @@ def run_serve(args):
             got += len(srv.poll(256, wait_ms=100))
     lat_s, lat_l, qms, done, checked, bad, edges, h2d, d2h = [], [], [], 0, 0, 0, 0, 0, 0
     pool_of = {}
+    lock = threading.Lock()
     stop = threading.Event()
     sent = [0]
 
@@ -483,7 +484,8 @@ def run_serve(args):
             if d > 0:
                 time.sleep(d)
             i = len(small) + int(rng.integers(len(large))) if rng.random() < 0.05 else int(rng.integers(len(small)))
-            pool_of[srv.submit(pool[i])] = i
+            with lock:   # a fast request can be polled before submit() returns here
+                pool_of[srv.submit(pool[i])] = i
             sent[0] += 1
         stop.set()
 
@@ -495,7 +497,8 @@ def run_serve(args):
     th.start()
     while not (stop.is_set() and done >= sent[0]):
         for r in srv.poll(1024, wait_ms=20):
-            i = pool_of.pop(r["ticket"], None)
+            with lock:
+                i = pool_of.pop(r["ticket"])
             done += 1
             if r["status"] != 0:
                 bad += 1
