@@ -34,13 +34,37 @@ struct Params {
 // Canonical labels of vertices tid+1, tid+1+n, ...: every vertex takes the
 // smallest member id of its SCC, which the update passes fold into
 // smin[representative].  Runs after the last pass barrier, so label and
-// smin are final.
+// smin are final.  Four vertices per thread and round: their label loads,
+// then their smin gathers, are issued back to back, so a thread waits on
+// two memory latencies per four vertices instead of two per vertex.  The
+// pointers carry no __restrict__: inside the SCC kernel label and smin were
+// written by other CTAs of the same launch and must not be read through the
+// non-coherent read-only path.
+constexpr uint32_t LABEL_UNROLL = 4;
+
+__device__ __forceinline__ void canon_labels(const uint32_t *label, const uint32_t *smin, uint32_t *out, uint32_t V,
+                                             uint32_t tid, uint32_t n)
+{
+    for (uint32_t v0 = tid + 1u; v0 <= V; v0 += LABEL_UNROLL * n) {
+        uint32_t l[LABEL_UNROLL];
+#pragma unroll
+        for (uint32_t j = 0; j < LABEL_UNROLL; ++j) {
+            const uint32_t v = v0 + j * n;
+            l[j] = v <= V ? label[v] : 0xFFFFFFFFu;
+        }
+#pragma unroll
+        for (uint32_t j = 0; j < LABEL_UNROLL; ++j) l[j] = l[j] <= V ? smin[l[j]] : 0u;
+#pragma unroll
+        for (uint32_t j = 0; j < LABEL_UNROLL; ++j) {
+            const uint32_t v = v0 + j * n;
+            if (v <= V) out[v - 1u] = l[j];
+        }
+    }
+}
+
 __device__ __forceinline__ void write_labels(const Work &w, uint32_t V, uint32_t *out, uint32_t tid, uint32_t n)
 {
-    for (uint32_t v = tid + 1u; v <= V; v += n) {
-        const uint32_t l = w.label[v];
-        out[v - 1u] = l <= V ? w.smin[l] : 0u;
-    }
+    canon_labels(w.label, w.smin, out, V, tid, n);
 }
 
 // ---------------------------------------------------------------------
@@ -107,12 +131,12 @@ __global__ void k_canon_write(const uint32_t *__restrict__ label, const uint32_t
                               uint32_t *__restrict__ out, uint32_t V, const Ctl *ctl)
 {
     if (ctl && ctl->labels_done) return;
-    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, n = gridDim.x * blockDim.x;
-    for (uint32_t v = tid + 1u; v <= V; v += n) {
-        uint32_t l = label[v];
-        out[v - 1u] = l <= V ? smin[l] : 0u;
-    }
+    canon_labels(label, smin, out, V, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
+
+// CTAs of 256 threads for k_canon_write: one round of LABEL_UNROLL vertices
+// per thread covers V.
+int canon_ctas(uint32_t V) { return (int)(((uint64_t)V + 256u * LABEL_UNROLL - 1u) / (256u * LABEL_UNROLL) + 1u); }
 
 // ---------------------------------------------------------------------
 // host side
@@ -438,8 +462,7 @@ extern "C" int scc_run(scc_context *ctx, const scc_csr_view *gv, int algo, uint3
     launches++;
     CK(cudaEventRecord(ctx->ev[2], st));
     if (dout) {
-        const int cb = std::min<int>(ctx->nsm * 8, (int)((V + 255) / 256) + 1);
-        k_canon_write<<<cb, 256, 0, st>>>(ctx->work.label, ctx->work.smin, dout, V, ctx->work.ctl);
+        k_canon_write<<<canon_ctas(V), 256, 0, st>>>(ctx->work.label, ctx->work.smin, dout, V, ctx->work.ctl);
         launches += 1;
         CK(cudaGetLastError());
         if (!dev) CK(cudaMemcpyAsync(labels_out, dout, (size_t)V * 4, cudaMemcpyDeviceToHost, st));
@@ -529,8 +552,7 @@ int sccb_launch_block_path(const Graph &g, const Work &w, int t1, int t2, int lw
     void *args[] = {&p};
     e = cudaLaunchKernel(fn, dim3(1), dim3(BLOCK_THREADS), args, smem, st);
     if (e != cudaSuccess) return cuda_status(e);
-    const int cb = (int)std::min<uint32_t>(1184u, (g.V + 255u) / 256u + 1u);
-    k_canon_write<<<cb, 256, 0, st>>>(w.label, w.smin, dout, g.V, nullptr);
+    k_canon_write<<<canon_ctas(g.V), 256, 0, st>>>(w.label, w.smin, dout, g.V, nullptr);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_status(e);
     *launches = 2;
