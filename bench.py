@@ -19,12 +19,19 @@ driver, labels canonicalised and written).
           device, SCC_FLAG_DERIVE_REVERSE) and the D2H copy of the labels are
           inside the timed region; e2e.both_csr_copied times the call that
           copies both CSRs.
-With --gpus N > 1 (torchrun) every rank runs an independent replica of the
-graph (the plain path does not shard); value = N * E / max-over-ranks time.
+  parity: the labels of the last timed step compared, vertex by vertex,
+          with the oracle's iterative Tarjan on the same graph (checker run
+          on rank 0 after the timed region).
+With --gpus N > 1 every rank runs an independent replica of the graph (the
+plain path does not shard); value = N * E / max-over-ranks time.  Launched
+without torchrun, bench.py starts the N ranks itself (torch.distributed.run
+on 127.0.0.1); under torchrun WORLD_SIZE must equal N.  --config cfg4 shards
+N x 4,096 graphs over the ranks by bytes instead.
 
 --impl reference times the reference's CPU-side answer for this path on the
 host cores: the reference has no CPU SCC implementation, so this is the
 project's iterative Tarjan oracle (one core, a full decomposition per step).
+That arm does not load the engine's library.
 """
 from __future__ import annotations
 
@@ -75,7 +82,8 @@ def _gen_graph(cfg: str, scale: int | None, device):
 
 class ClockSampler:
     """SM clock and throttle reasons sampled every ~2 ms during the timed
-    region (NVML, the library nvidia-smi reads; falls back to nvidia-smi)."""
+    region through NVML (read-only queries; the library nvidia-smi reads).
+    Without NVML the record says so and holds no samples."""
 
     REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
                "sw_power_cap": 0x4}
@@ -121,6 +129,33 @@ class ClockSampler:
         reasons = sorted(k for k, bit in self.REASONS.items() if mask & bit)
         return {"sm_mhz": statistics.median(c for c, _ in self.samples), "sm_max_mhz": self.max_mhz,
                 "reasons": reasons, "samples": len(self.samples), "source": "nvml"}
+
+
+def _host_cpu():
+    """CPU model and thread counts of the host the CPU baseline ran on."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    try:
+        usable = len(os.sched_getaffinity(0))
+    except AttributeError:  # pragma: no cover
+        usable = os.cpu_count()
+    return {"cpu_model": model, "nproc": os.cpu_count(), "usable_threads": usable}
+
+
+def _config_dict(cfg_name: str, scale, V: int, E: int, world: int) -> dict:
+    """The workload description both arms print (same keys and values)."""
+    cfg = CONFIGS[cfg_name]
+    return {"workload": f"{cfg_name}: {cfg['desc']}" + (f" [scale override {scale}]" if scale else ""),
+            "V": V, "E": E, "seed": 1, "algo": cfg["algo"], "t1": cfg["t1"], "t2": cfg["t2"],
+            "warp": cfg["warp"], "l2": "flushed before every step (256 MiB write)",
+            "parallelism": "replicas" if world > 1 else "single GPU"}
 
 
 def _peak_hbm():
@@ -253,6 +288,7 @@ def run_ours(args):
     t_e2e_both, lab_both = e2e_leg(False)
     t_e2e, lab_fwd = e2e_leg(True)
     assert np.array_equal(lab_both, lab_fwd)
+    assert np.array_equal(lab_fwd, labels.cpu().numpy().view(np.uint32))
 
     B_alg = 8 * ins["edges_scanned"] + 12 * ins["vertex_visits"]
     peak, peak_kind = _peak_hbm()
@@ -271,10 +307,7 @@ def run_ours(args):
         "vs_baseline": None,
         "dtype": "u32",
         "data": "synthetic (seeded generator, no dataset)",
-        "config": {"workload": f"{args.config}: {cfg['desc']}" + (f" [scale override {args.scale}]" if args.scale else ""),
-                   "V": V, "E": E, "seed": 1, "algo": cfg["algo"], "t1": cfg["t1"], "t2": cfg["t2"],
-                   "warp": cfg["warp"], "l2": "flushed before every step (256 MiB write)",
-                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "config": _config_dict(args.config, args.scale, V, E, world),
         "num_sccs": int(res.num_sccs),
         "counts": {"trim1": int(res.num_trim1), "trim2": int(res.num_trim2), "pivot": int(res.num_pivot)},
         "passes": res.stats["passes"], "outer_iters": res.stats["outer_iters"],
@@ -299,14 +332,24 @@ def run_ours(args):
         "gpu_launches": int(launches),
         "clocks": clk,
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        from oracle import oracle
-        hFr_np, hFc_np = hg.Fr, hg.Fc
-        t_cpu, reps = oracle.time_tarjan(V, hFr_np, hFc_np, budget_s=20.0, max_reps=3)
-        out["cpu_baseline"] = {"value": round(E / t_cpu / 1e6, 2), "unit": "Medges/s", "cores": 1,
-                               "kind": "port", "sample": f"full graph, iterative Tarjan, median of {reps} run(s), "
-                                                         f"{t_cpu:.2f} s per run"}
     if rank == 0:
+        # checker and CPU baseline (after the timed region): the oracle's
+        # iterative Tarjan on the same host CSR
+        from oracle import oracle
+        if not args.no_parity:
+            ref_lab, ref_n = oracle.tarjan(V, hg.Fr, hg.Fc)
+            got = labels.cpu().numpy().view(np.uint32)
+            nbad = int(np.count_nonzero(got != ref_lab[1:]))
+            out["parity"] = nbad == 0 and int(res.num_sccs) == ref_n
+            out["parity_detail"] = {"against": "oracle iterative Tarjan (canonical min-id labels)",
+                                    "labels_checked": V, "labels_differing": nbad, "num_sccs_oracle": ref_n,
+                                    "labels_of": "last timed step; the e2e legs' labels equal them"}
+        if world == 1 and not args.no_cpu_baseline:
+            t_cpu, reps = oracle.time_tarjan(V, hg.Fr, hg.Fc, budget_s=20.0, max_reps=3)
+            out["cpu_baseline"] = {"value": round(E / t_cpu / 1e6, 2), "unit": "Medges/s", "cores": 1,
+                                   "kind": "port", "sample": f"full graph, iterative Tarjan, median of {reps} "
+                                                             f"run(s), {t_cpu:.2f} s per run",
+                                   "host": _host_cpu()}
         print(json.dumps(out), flush=True)
     eng.close()
     if world > 1:
@@ -427,7 +470,8 @@ def run_batch(args):
         t_cpu = time.perf_counter() - t0
         out["cpu_baseline"] = {"value": round(len(sample) / t_cpu, 1), "unit": "graphs/s", "cores": cores,
                                "kind": "port", "sample": f"first {len(sample)} graphs of the mix, iterative "
-                                                         f"Tarjan per graph on a {cores}-thread pool"}
+                                                         f"Tarjan per graph on a {cores}-thread pool",
+                               "host": _host_cpu()}
     if rank == 0:
         print(json.dumps(out), flush=True)
     b.close()
@@ -550,13 +594,21 @@ def run_reference(args):
         return
     import torch
 
-    from detectingscc_b200 import graphs
+    from detectingscc_b200 import graphs   # the seeded generators (PyTorch only; the engine is not loaded)
     from oracle import oracle
+    from oracle.gtgraph_ref import build_csr
     cfg = CONFIGS[args.config]
     if args.config in ("cfg4", "cfg5"):
         # both are many independent graphs of the cfg4 mix: Tarjan per graph on all host cores
         import concurrent.futures as cf
-        gs = _batch_graphs(args.scale or 4096, seed=1)
+        from types import SimpleNamespace
+
+        def mk(i):
+            V, s_, d_ = graphs.batch_mix_graph(i, seed=1)
+            Fr, Fc, _, _ = build_csr(V, s_, d_)
+            return SimpleNamespace(V=V, Fr=Fr, Fc=Fc)
+        with cf.ThreadPoolExecutor(os.cpu_count() or 1) as ex:
+            gs = list(ex.map(mk, range(args.scale or 4096)))
         cores = os.cpu_count() or 1
         sample = gs[: max(64, len(gs) // 8)]
         times = []
@@ -574,7 +626,8 @@ def run_reference(args):
                           "config": {"workload": f"{args.config}: {cfg['desc']}", "graphs": len(gs)},
                           "cpu_baseline": {"value": v, "unit": "graphs/s", "cores": cores, "kind": "port",
                                            "sample": f"first {len(sample)} graphs per step, Tarjan per graph on a "
-                                                     f"{cores}-thread pool (the reference has no CPU SCC path)"},
+                                                     f"{cores}-thread pool (the reference has no CPU SCC path)",
+                                           "host": _host_cpu()},
                           "e2e": {"value": v, "unit": "graphs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
               flush=True)
         return
@@ -597,10 +650,10 @@ def run_reference(args):
         "value": v, "unit": "Medges/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(t * 1e3, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u32", "data": "synthetic (seeded generator, no dataset)",
-        "config": {"workload": f"{args.config}: {cfg['desc']}", "V": V, "E": E, "seed": 1},
+        "config": _config_dict(args.config, args.scale, V, E, world),
         "cpu_baseline": {"value": v, "unit": "Medges/s", "cores": 1, "kind": "port",
                          "sample": "full graph per step; the reference has no CPU SCC path, so this is the "
-                                   "project's iterative Tarjan oracle on one host core"},
+                                   "project's iterative Tarjan oracle on one host core", "host": _host_cpu()},
         "e2e": {"value": v, "unit": "Medges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     ref_gpu = _reference_gpu_time(args, V, E, Fr, Fc, Br, Bc, cfg)
@@ -616,13 +669,17 @@ def _reference_gpu_time(args, V, E, Fr, Fc, Br, Bc, cfg):
     import re
     import tempfile
 
-    import detectingscc_b200 as scc
     ref = os.path.join(ROOT, "oracle", "_ref", "scc_ref")
     if not os.path.exists(ref):
         return None
     with tempfile.TemporaryDirectory() as td:
         path = os.path.join(td, "graph.bin")
-        scc.save_binary(path, scc.Graph(V, E, Fr, Fc, Br, Bc))
+        # the binary CSR both loaders read: "SCCBIN01", u64 V, u64 E, Fr, Fc, Br, Bc (u32)
+        with open(path, "wb") as f:
+            f.write(b"SCCBIN01")
+            f.write(np.array([V, E], dtype=np.uint64).tobytes())
+            for a in (Fr, Fc, Br, Bc):
+                f.write(np.ascontiguousarray(a, dtype=np.uint32).tobytes())
         runs = []
         for _ in range(3):
             try:
@@ -642,6 +699,19 @@ def _reference_gpu_time(args, V, E, Fr, Fc, Br, Bc, cfg):
                     "cudaMalloc + H2D; best of 3"}
 
 
+def _launch_ranks(n: int) -> int:
+    """Starts n ranks of this same command (torch.distributed.run on
+    127.0.0.1, one process per GPU) and returns their exit status."""
+    import socket
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr=127.0.0.1", f"--master-port={port}", os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -651,7 +721,14 @@ def main():
     ap.add_argument("--config", default="cfg2", choices=sorted(CONFIGS))
     ap.add_argument("--scale", type=int, default=None, help="smaller graph (profiling aid, not a bench value)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true", help="skip the label check against the oracle")
     args = ap.parse_args()
+    world = os.environ.get("WORLD_SIZE")
+    if world is None and args.gpus > 1:
+        sys.exit(_launch_ranks(args.gpus))
+    if world is not None and int(world) != args.gpus:
+        print(f"bench.py: --gpus {args.gpus} but WORLD_SIZE={world}; launch one rank per GPU", file=sys.stderr)
+        sys.exit(2)
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.impl == "reference":

@@ -14,6 +14,7 @@ process (e.g. PyTorch) has loaded.
 """
 from __future__ import annotations
 
+import concurrent.futures as cf
 import os
 import subprocess
 import sys
@@ -53,7 +54,7 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> str:
     os.makedirs(os.path.dirname(CLI), exist_ok=True)
     hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [
         os.path.join(ROOT, "include", "scc_b200.h"), os.path.join(ROOT, "include", "scc_compat.h")]
-    objs = []
+    objs, jobs = [], []
     for src in CU_SOURCES:
         s = os.path.join(CSRC, src)
         if not os.path.exists(s):
@@ -61,8 +62,12 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> str:
         o = os.path.join(BUILD, src + ".o")
         if force or _newer(o, [s] + hdrs):
             extra = ["-Xptxas", "-v"] if verbose_ptxas else []
-            _run([NVCC] + CU_FLAGS + extra + ["-c", s, "-o", o])
+            jobs.append([NVCC] + CU_FLAGS + extra + ["-c", s, "-o", o])
         objs.append(o)
+    # the translation units are independent: compile them concurrently
+    with cf.ThreadPoolExecutor(max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(_run, j) for j in jobs]:
+            f.result()
     lib_objs = []
     for src in CXX_LIB_SOURCES + CXX_CLI_SOURCES:
         s = os.path.join(CSRC, src)

@@ -113,10 +113,14 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_scc_batch(BatchPara
             if (cr == 0 && threadIdx.x == 0) s_kb = atomicAdd(&p.next[0], 1u);
             cluster_barrier();
             const uint32_t k = *cooperative_groups::this_cluster().map_shared_rank(&s_kb, 0);
+            // check mode: every graph starts from a clean software barrier
+            // word (all CTAs are past the previous graph here; a graph that
+            // ended on a timed-out wait can leave the word mid-count)
+            if (p.cbar && cr == 0 && threadIdx.x == 0) p.cbar[(blockIdx.x - cr) / cn] = 0u;
             cluster_barrier();   // rank 0 rewrites s_kb only after every CTA has read it
             if (k >= p.nbig) break;
             ClusterExec<false> ex{nullptr, 0u, cr, cn, p.cbar ? p.cbar + (blockIdx.x - cr) / cn : nullptr,
-                                  p.timeout_ns};
+                                  p.timeout_ns, p.pass_cap, p.cbar ? p.hold : 0u};
             batch_one<HONG>(ex, p, p.order[k], lead, s_w);
         }
     }
@@ -126,7 +130,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_scc_batch(BatchPara
         __syncthreads();
         const uint32_t k = s_k;
         if (k >= p.n) return;
-        BlockExec<false> ex{nullptr, 0u};
+        BlockExec<false> ex{nullptr, 0u, p.pass_cap};
         batch_one<HONG>(ex, p, p.order[k], mine, s_w);
     }
 }
@@ -157,9 +161,14 @@ size_t sccb_batch_smem(int threads, uint32_t qcap) { return batch_smem(threads, 
 int sccb_batch_ctas(int threads, uint32_t qcap, int nsm, uint32_t *out, int cluster)
 {
     const size_t smem = batch_smem(threads, qcap);
+    // the limit covers the largest staging slice a schedule may use (768
+    // entries, capped at 200 KB), so batches, autotuning and server lanes on
+    // other host threads never lower it under one another
+    const size_t smem_max = std::min<size_t>(batch_smem(threads, 768), 200 * 1024);
+    if (smem > smem_max) return SCC_ERR_INVALID_ARG;
     for (int h = 0; h < 4; h++) {
         void *fn = pick_batch_kernel(threads, (h & 1) != 0, h >= 2);
-        if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+        if (sccb_smem_limit(fn, smem_max) != SCC_OK ||
             (cluster > 8 && cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)) {
             cudaGetLastError();
             return SCC_ERR_CUDA;
@@ -283,7 +292,7 @@ struct scc_batch {
     // captured launch
     cudaGraphExec_t gexec = nullptr;
     int g_algo = 0, g_w = 0, g_threads = 0, g_cluster = 0, g_check = 0;
-    uint32_t g_flags = 0, g_qcap = 0, g_big = 0;
+    uint32_t g_flags = 0, g_qcap = 0, g_big = 0, g_cap = 0, g_hold = 0, g_timeout = 0;
 };
 
 static void batch_free(scc_batch *b)
@@ -513,13 +522,15 @@ extern "C" int scc_batch_run(scc_batch *b, int algo, uint32_t flags, int warp_wi
         const uint32_t keyflags = flags & (SCC_FLAG_TRIM1 | SCC_FLAG_TRIM2);
         if (!b->gexec || b->g_algo != algo || b->g_flags != keyflags || b->g_w != warp_width ||
             b->g_threads != b->threads || b->g_qcap != b->qcap || b->g_cluster != b->cluster ||
-            b->g_big != b->big_vertices || b->g_check != b->ctx->cluster_check) {
+            b->g_big != b->big_vertices || b->g_check != b->ctx->cluster_check || b->g_cap != b->ctx->max_passes ||
+            b->g_hold != b->ctx->hold_pass || b->g_timeout != b->ctx->timeout_ms) {
             if (b->gexec) { cudaGraphExecDestroy(b->gexec); b->gexec = nullptr; }
             BatchParams p{b->dgraphs, b->dorder, b->n, b->dFr, b->dFc, b->dBr, b->dBc, 0u, b->dout, b->dres,
                           b->scratch, (unsigned long long)b->scratch_per_cta, b->dnext, b->nbig,
                           b->ctx->cluster_check && b->cluster > 1 ? b->dcbar : nullptr, 1u, nullptr, b->qcap, b->ctx->bu_k,
                           (flags & SCC_FLAG_TRIM1) ? 1 : 0, (flags & SCC_FLAG_TRIM2) ? 1 : 0, lw,
-                          (unsigned long long)b->ctx->timeout_ms * 1000000ull};
+                          (unsigned long long)b->ctx->timeout_ms * 1000000ull, b->ctx->max_passes,
+                          b->ctx->hold_pass};
             cudaGraph_t graph = nullptr;
             if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
                 cudaGetLastError();
@@ -537,6 +548,9 @@ extern "C" int scc_batch_run(scc_batch *b, int algo, uint32_t flags, int warp_wi
             b->g_algo = algo; b->g_flags = keyflags; b->g_w = warp_width;
             b->g_threads = b->threads; b->g_qcap = b->qcap; b->g_cluster = b->cluster; b->g_big = b->big_vertices;
             b->g_check = b->ctx->cluster_check;
+            b->g_cap = b->ctx->max_passes;
+            b->g_hold = b->ctx->hold_pass;
+            b->g_timeout = b->ctx->timeout_ms;
         }
         if (cudaGraphLaunch(b->gexec, b->stream) != cudaSuccess) { cudaGetLastError(); return SCC_ERR_CUDA; }
         cudaEventRecord(b->ev[1], b->stream);

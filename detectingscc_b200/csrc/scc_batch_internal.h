@@ -38,6 +38,8 @@ struct BatchParams {
     uint32_t qcap, bu_k;
     int t1, t2, lw;
     unsigned long long timeout_ns;
+    uint32_t pass_cap;          // per graph: passes after which the graph fails with SCC_ERR_NOT_CONVERGED (0: none)
+    uint32_t hold;              // check mode: failure-detection test hook (ClusterExec::barrier), 0: off
 };
 
 // Shared memory of the batch kernel for a CTA size and staging slice.

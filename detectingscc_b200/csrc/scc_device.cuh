@@ -197,7 +197,9 @@ struct GridExec {
     static constexpr bool instr = INSTR;
     static constexpr bool grid = true;
     Ctl *ctl;
-    unsigned gl;   // pass counter, identical in every thread
+    unsigned gl;        // pass counter, identical in every thread
+    unsigned cap = 0;   // pass cap of the run (0: none), see run_pass
+    unsigned hold = 0;  // failure-detection test hook, see sync
     __device__ __forceinline__ unsigned tid() const { return blockIdx.x * blockDim.x + threadIdx.x; }
     __device__ __forceinline__ unsigned nthr() const { return gridDim.x * blockDim.x; }
     __device__ __forceinline__ unsigned wid() const { return tid() >> 5; }
@@ -210,6 +212,11 @@ struct GridExec {
     // waiter leaves early when the sticky error word (polled with the
     // counter in one 8-byte load) is set, or after ctl->timeout_ns; any CTA
     // that sees an error returns, and the error stays set for the others.
+    //
+    // hold = k + 1 makes the last CTA withhold its arrival at pass k: the
+    // failure-detection tests use it to make every wait of that barrier run
+    // out (an arrival that never comes), which must end the run with
+    // E_TIMEOUT and leave the context usable.
     __device__ bool sync(const unsigned *snap = nullptr)
     {
         __shared__ int s_err;
@@ -217,7 +224,10 @@ struct GridExec {
         if (threadIdx.x == 0) {
             const unsigned nb = (blockIdx.x == 0) ? (0x80000000u - (gridDim.x - 1u)) : 1u;
             unsigned old;
-            asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(&ctl->bar_count), "r"(nb) : "memory");
+            if (hold != 0u && gl + 1u == hold && blockIdx.x == gridDim.x - 1u)
+                asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(old) : "l"(&ctl->bar_count) : "memory");
+            else
+                asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(&ctl->bar_count), "r"(nb) : "memory");
             int err = 0;
             unsigned long long t0 = 0;
             for (unsigned spin = 0;; spin++) {
@@ -249,6 +259,7 @@ struct BlockExec {
     static constexpr bool grid = false;
     Ctl *ctl;
     unsigned gl;
+    unsigned cap = 0;
     __device__ __forceinline__ unsigned tid() const { return threadIdx.x; }
     __device__ __forceinline__ unsigned nthr() const { return blockDim.x; }
     __device__ __forceinline__ unsigned wid() const { return threadIdx.x >> 5; }
@@ -306,6 +317,8 @@ struct ClusterExec {
     unsigned rank, csize;
     unsigned *soft;   // the cluster's barrier counter, or nullptr for the hardware barrier
     unsigned long long soft_timeout_ns;
+    unsigned cap = 0;
+    unsigned hold = 0;  // check mode only: the last CTA withholds its arrival at pass hold - 1 (test hook)
     __device__ __forceinline__ unsigned tid() const { return rank * blockDim.x + threadIdx.x; }
     __device__ __forceinline__ unsigned nthr() const { return csize * blockDim.x; }
     __device__ __forceinline__ unsigned wid() const { return tid() >> 5; }
@@ -321,7 +334,10 @@ struct ClusterExec {
         if (threadIdx.x == 0) {
             const unsigned nb = rank == 0 ? (0x80000000u - (csize - 1u)) : 1u;
             unsigned old;
-            asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(soft), "r"(nb) : "memory");
+            if (hold != 0u && gl + 1u == hold && rank == csize - 1u)
+                asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(old) : "l"(soft) : "memory");
+            else
+                asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(soft), "r"(nb) : "memory");
             unsigned long long t0 = 0;
             for (unsigned spin = 0;; spin++) {
                 unsigned v;
@@ -356,9 +372,19 @@ struct ClusterExec {
 // body with (cur, nxt) counter slots, then the barrier.  A pass pushes into
 // counter slot gl%3 and buffer parity gl&1; the following pass reads them as
 // its "current" slot (gl+2)%3 and parity (gl+1)&1.
+//
+// A run whose pass count reaches ex.cap (when set) stops with
+// E_NOT_CONVERGED: the host's bound on the work of one run, on top of the
+// V + 2 passes every convergence loop allows itself.
 template <class Ex, class F>
 __device__ __forceinline__ bool run_pass(Ex &ex, int phase, F &&body)
 {
+    if (ex.cap != 0u && ex.gl >= ex.cap) {
+        if (ex.leader()) set_error(ex.ctl, E_NOT_CONVERGED, 70);
+        ex.sync();
+        ex.gl++;
+        return false;
+    }
     const unsigned nxt = ex.gl % 3u, clr = (ex.gl + 1u) % 3u, cur = (ex.gl + 2u) % 3u;
     if (ex.leader()) {
 #pragma unroll

@@ -29,6 +29,8 @@ struct Params {
     int t1, t2, lw;
     uint32_t tail_n;
     uint32_t *out;      // canonical labels (device, V entries) written at the end of the run, or nullptr
+    uint32_t pass_cap;  // passes after which the run stops with SCC_ERR_NOT_CONVERGED (0: no cap)
+    uint32_t hold;      // failure-detection test hook (GridExec::sync), 0: off
 };
 
 // Canonical labels of vertices tid+1, tid+1+n, ...: every vertex takes the
@@ -84,7 +86,7 @@ __global__ void __launch_bounds__(GRID_THREADS, 1) k_scc_grid(Params p)
     if (*(volatile int *)&p.w.ctl->error) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) p.w.ctl->t_start = gtimer();
     bq_init();
-    GridExec<INSTR> ex{p.w.ctl, 0u};
+    GridExec<INSTR> ex{p.w.ctl, 0u, p.pass_cap, p.hold};
     Carry cy{0u, 0u, 0u};
     int rc = HONG ? hong_front(ex, p.g, p.w, p.t1, p.t2, p.lw, cy) : slota_front(ex, p.g, p.w, p.t1, p.lw, cy);
     if (rc == RUN_DONE) rc = HONG ? hong_loop(ex, p.g, p.w, cy, p.tail_n) : slota_peels(ex, p.g, p.w, cy, p.tail_n);
@@ -92,7 +94,7 @@ __global__ void __launch_bounds__(GRID_THREADS, 1) k_scc_grid(Params p)
         // the live set is small: CTA 0 finishes alone with block barriers
         if (blockIdx.x != 0) return;
         if (threadIdx.x == 0) { p.w.ctl->tail_pass = cy.gl; p.w.ctl->nlive_tail = cy.nL; }
-        BlockExec<INSTR> bx{p.w.ctl, cy.gl};
+        BlockExec<INSTR> bx{p.w.ctl, cy.gl, p.pass_cap};
         if (HONG) hong_loop(bx, p.g, p.w, cy, 0u);
         else slota_peels(bx, p.g, p.w, cy, 0u);
         if (threadIdx.x == 0) p.w.ctl->passes = bx.gl;
@@ -113,7 +115,7 @@ __global__ void __launch_bounds__(BLOCK_THREADS, 1) k_scc_block(Params p)
     if (*(volatile int *)&p.w.ctl->error) return;
     if (threadIdx.x == 0) p.w.ctl->t_start = gtimer();
     bq_init();
-    BlockExec<INSTR> ex{p.w.ctl, 0u};
+    BlockExec<INSTR> ex{p.w.ctl, 0u, p.pass_cap};
     Carry cy{0u, 0u, 0u};
     int rc = HONG ? hong_front(ex, p.g, p.w, p.t1, p.t2, p.lw, cy) : slota_front(ex, p.g, p.w, p.t1, p.lw, cy);
     if (rc == RUN_DONE) rc = HONG ? hong_loop(ex, p.g, p.w, cy, 0u) : slota_peels(ex, p.g, p.w, cy, 0u);
@@ -335,16 +337,38 @@ extern "C" int scc_destroy(scc_context *ctx)
     return SCC_OK;
 }
 
-// Sets the kernel's dynamic shared memory limit (every call: other callers
-// of the same kernel may have set a lower one) and returns the grid of its
-// cooperative launch, computed once per (kernel, shared memory, CTA cap).
-// Returns 0 on failure.
+// Raises the dynamic shared memory limit of kernel fn on the current device
+// to max_bytes, once per (device, kernel), under one process-wide lock.  The
+// limit only ever goes up and every caller passes the largest size any of
+// its launches of fn can request, so a launch on one host thread can never
+// find the limit lowered by another thread between its check and its launch.
+int sccb_smem_limit(void *fn, size_t max_bytes)
+{
+    static std::mutex mu;
+    struct Done { int dev; void *fn; };
+    static Done done[256];
+    static int ndone = 0;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) { cudaGetLastError(); return SCC_ERR_CUDA; }
+    std::lock_guard<std::mutex> lock(mu);
+    for (int i = 0; i < ndone; i++)
+        if (done[i].dev == dev && done[i].fn == fn) return SCC_OK;
+    const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_bytes);
+    if (e != cudaSuccess) { cudaGetLastError(); return cuda_status(e); }
+    if (ndone < 256) done[ndone++] = Done{dev, fn};
+    return SCC_OK;
+}
+
+// Largest dynamic shared memory of the plain-path kernels: the staging
+// slice is at most 768 entries (scc_set_tuning "qcap").
+static size_t max_plain_smem() { return dyn_smem_bytes(768); }
+
+// Makes sure the kernel's dynamic shared memory limit covers every launch
+// of it and returns the grid of its cooperative launch, computed once per
+// (kernel, shared memory, CTA cap).  Returns 0 on failure.
 static int prepare_kernel(scc_context *ctx, void *fn, size_t smem, int threads)
 {
-    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
-        cudaGetLastError();
-        return 0;
-    }
+    if (smem > max_plain_smem() || sccb_smem_limit(fn, max_plain_smem()) != SCC_OK) return 0;
     for (int i = 0; i < ctx->n_prepared; i++) {
         const scc_context::Prepared &q = ctx->prepared[i];
         if (q.fn == fn && q.smem == smem && q.cap == ctx->max_blocks_per_sm) return q.nblocks;
@@ -440,7 +464,7 @@ extern "C" int scc_run(scc_context *ctx, const scc_csr_view *gv, int algo, uint3
     ctx->work.bu_k = ctx->bu_k;
     const size_t smem = dyn_smem_bytes(ctx->qcap);
     Params p{g, ctx->work, (flags & SCC_FLAG_TRIM1) ? 1 : 0, (flags & SCC_FLAG_TRIM2) ? 1 : 0, lw, ctx->tail_vertices,
-             dout};
+             dout, ctx->max_passes, ctx->hold_pass};
     bool use_block = (V <= ctx->block_max_vertices && E <= ctx->block_max_edges);
     if (flags & SCC_FLAG_FORCE_GRID) use_block = false;
     if (flags & SCC_FLAG_FORCE_BLOCK) use_block = true;
@@ -503,6 +527,8 @@ extern "C" int scc_set_tuning(scc_context *ctx, const char *key, long long value
     else if (!strcmp(key, "max_blocks_per_sm")) ctx->max_blocks_per_sm = (int)value;
     else if (!strcmp(key, "bu_k")) ctx->bu_k = (uint32_t)value;
     else if (!strcmp(key, "cluster_check")) ctx->cluster_check = value ? 1 : 0;
+    else if (!strcmp(key, "max_passes")) ctx->max_passes = (uint32_t)value;
+    else if (!strcmp(key, "test_withhold_arrival")) ctx->hold_pass = (uint32_t)value;
     else if (!strcmp(key, "qcap")) {
         if (value < 32 || value > 768) return SCC_ERR_INVALID_ARG;
         ctx->qcap = (uint32_t)value;
@@ -546,11 +572,12 @@ int sccb_launch_block_path(const Graph &g, const Work &w, int t1, int t2, int lw
 {
     const size_t smem = dyn_smem_bytes(w.qcap);
     void *fn = pick_block(false, hong);
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return cuda_status(e);
-    Params p{g, w, t1, t2, lw, 0u};
+    if (smem > max_plain_smem()) return SCC_ERR_INVALID_ARG;
+    const int rc = sccb_smem_limit(fn, max_plain_smem());
+    if (rc != SCC_OK) return rc;
+    Params p{g, w, t1, t2, lw, 0u, nullptr, 0u, 0u};
     void *args[] = {&p};
-    e = cudaLaunchKernel(fn, dim3(1), dim3(BLOCK_THREADS), args, smem, st);
+    cudaError_t e = cudaLaunchKernel(fn, dim3(1), dim3(BLOCK_THREADS), args, smem, st);
     if (e != cudaSuccess) return cuda_status(e);
     k_canon_write<<<canon_ctas(g.V), 256, 0, st>>>(w.label, w.smin, dout, g.V, nullptr);
     e = cudaGetLastError();

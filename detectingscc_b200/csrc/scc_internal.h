@@ -41,6 +41,9 @@ struct scc_context {
     uint32_t qcap = 512;                 // per-warp staging slice entries (2 queues x 32 warps in shared memory)
     uint32_t bu_k = 2;                   // bottom-up BFS step when frontier edges > bu_k * scope (0 = off)
     int cluster_check = 0;               // batched launches: bounded software cluster barriers (check mode)
+    uint32_t max_passes = 0;             // a run stops with SCC_ERR_NOT_CONVERGED after this many passes (0: no cap)
+    uint32_t hold_pass = 0;              // failure-detection test hook: k + 1 = one CTA withholds its barrier
+                                         // arrival at pass k (grid launches; batched launches in check mode)
 
     // grid size of the cooperative launch (occupancy x SMs) per kernel and
     // shared memory size, computed once
@@ -62,3 +65,6 @@ int sccb_derive_reverse(scc_context *ctx, const uint32_t *dFr, const uint32_t *d
                         uint32_t *dBr, uint32_t *dBc, sccb::Ctl *ctl, cudaStream_t st);
 // Bytes of the workspace scc_ctx_reserve allocates for a graph.
 size_t scc_ctx_ws_need(uint32_t V, uint32_t E);
+// Raises kernel fn's dynamic shared memory limit on the current device to
+// max_bytes once (process-wide lock); returns an scc_status.
+int sccb_smem_limit(void *fn, size_t max_bytes);

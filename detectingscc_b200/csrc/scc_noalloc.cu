@@ -16,7 +16,11 @@
 //     that loads the library holds it until the process exits;
 //   * on the first call on a device, with that device current, the call
 //     looks up the device address of the array (cudaGetSymbolAddress) and
-//     caches it; make that first call before any stream capture;
+//     caches it per CUDA context (a context created later, e.g. after
+//     cudaDeviceReset, gets its own lookup); make that first call before
+//     any stream capture;
+//   * flags other than SCC_FLAG_DEVICE (required), SCC_FLAG_TRIM1 and
+//     SCC_FLAG_TRIM2 are rejected;
 //   * every call shares the one array and overwrites it: calls whose work
 //     overlaps on the GPU (different streams, threads) race and must be
 //     serialised by the caller;
@@ -56,26 +60,69 @@ constexpr size_t NOALLOC_BYTES = scratch_bytes(SCC_NOALLOC_MAX_VERTICES, SCC_NOA
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
 
-constexpr int MAX_DEVICES = 64;
 std::mutex g_mu;
-void *g_scratch_addr[MAX_DEVICES] = {};
 
-// Device address of the scratch array on the current device (looked up
-// once per device).  In host code the array's name is only a host-side
-// stand-in; kernels must be given this address.
-int scratch_address(int dev, char **out)
+// Unique id of the calling thread's current CUDA context, 0 when there is
+// none yet or the driver cannot tell.  The two driver entry points are
+// fetched through the runtime, so the library needs no link-time libcuda.
+unsigned long long current_ctx_id()
+{
+    using GetCurrent = int (*)(void **);
+    using GetId = int (*)(void *, unsigned long long *);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static bool tried = false;
+    if (!tried) {   // under g_mu
+        tried = true;
+        void *f = nullptr, *h = nullptr;
+        cudaDriverEntryPointQueryResult q1 = cudaDriverEntryPointSymbolNotFound, q2 = q1;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q1) == cudaSuccess &&
+            cudaGetDriverEntryPoint("cuCtxGetId", &h, cudaEnableDefault, &q2) == cudaSuccess &&
+            q1 == cudaDriverEntryPointSuccess && q2 == cudaDriverEntryPointSuccess && f && h) {
+            get_current = (GetCurrent)f;
+            get_id = (GetId)h;
+        }
+        cudaGetLastError();
+    }
+    void *c = nullptr;
+    unsigned long long id = 0;
+    if (get_current && get_id && get_current(&c) == 0 && c && get_id(c, &id) == 0) return id;
+    return 0;
+}
+
+struct AddrEntry {
+    unsigned long long ctx;
+    void *addr;
+};
+constexpr int MAX_CTX = 64;
+AddrEntry g_addr[MAX_CTX] = {};
+int g_naddr = 0;
+
+// Device address of the scratch array in the current context (looked up
+// once per context: the first call on a device, with that device current).
+// In host code the array's name is only a host-side stand-in; kernels must
+// be given this address.
+int scratch_address(char **out)
 {
     std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_scratch_addr[dev]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
-            cudaGetLastError();
-            return SCC_ERR_CUDA;
+    unsigned long long id = current_ctx_id();
+    if (id) {
+        for (int i = 0; i < g_naddr; i++) {
+            if (g_addr[i].ctx == id) {
+                *out = (char *)g_addr[i].addr;
+                return SCC_OK;
+            }
         }
-        g_scratch_addr[dev] = p;
     }
-    *out = (char *)g_scratch_addr[dev];
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+        cudaGetLastError();
+        return SCC_ERR_CUDA;
+    }
+    if (!id) id = current_ctx_id();   // the lookup above made the primary context current
+    if (id) g_addr[g_naddr < MAX_CTX ? g_naddr++ : (int)(id % MAX_CTX)] = AddrEntry{id, p};
+    *out = (char *)p;
     return SCC_OK;
 }
 
@@ -95,6 +142,7 @@ extern "C" int scc_run_noalloc(const scc_csr_view *gv, int algo, uint32_t flags,
     if (stats) memset(stats, 0, sizeof(*stats));
     if (!gv || !labels_out) return SCC_ERR_INVALID_ARG;
     if (!(flags & SCC_FLAG_DEVICE)) return SCC_ERR_INVALID_ARG;   // host inputs would need a device copy
+    if (flags & ~(SCC_FLAG_DEVICE | SCC_FLAG_TRIM1 | SCC_FLAG_TRIM2)) return SCC_ERR_INVALID_ARG;
     const bool hong = algo == SCC_ALGO_VHONG || algo == SCC_ALGO_WHONG;
     const bool warped = algo == SCC_ALGO_WHONG || algo == SCC_ALGO_WSLOTA;
     if (!hong && algo != SCC_ALGO_VSLOTA && algo != SCC_ALGO_WSLOTA) return SCC_ERR_INVALID_ARG;
@@ -115,12 +163,12 @@ extern "C" int scc_run_noalloc(const scc_csr_view *gv, int algo, uint32_t flags,
     if (V == 0) return SCC_OK;
     if (!gv->Fr || !gv->Br || (E && (!gv->Fc || !gv->Bc))) return SCC_ERR_INVALID_ARG;
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) {
+    if (cudaGetDevice(&dev) != cudaSuccess) {
         cudaGetLastError();
         return SCC_ERR_NO_DEVICE;
     }
     char *base = nullptr;
-    int rc = scratch_address(dev, &base);
+    int rc = scratch_address(&base);
     if (rc != SCC_OK) return rc;
 
     // carve the scratch exactly as scratch_bytes() counts it

@@ -303,7 +303,7 @@ int run_job(scc_server *s, Lane *L, Job &j, double t_start, std::vector<char> &a
                   (unsigned long long)carve_work(nullptr, j.maxV, j.maxE, true, nullptr), L->dnext, nbig, nullptr,
                   j.large ? (uint32_t)cluster : 1u, L->hdone, s->cfg.qcap, 2u, (s->cfg.flags & SCC_FLAG_TRIM1) ? 1 : 0,
                   (s->cfg.flags & SCC_FLAG_TRIM2) ? 1 : 0, lw_of(s->cfg.algo, s->cfg.warp_width),
-                  4000ull * 1000000ull};
+                  4000ull * 1000000ull, 0u, 0u};
     double t1 = now_ms();
     L->prof[Lane::P_UPLOAD] += t1 - t0;
     cudaEventRecord(L->k0, st);

@@ -10,7 +10,8 @@ GPU); a graph is reproducible for a given (seed, device).  Vertex ids are
                       duplicates kept, as a GTgraph random graph may hold
                       them) plus 16 planted directed cycles of length 4-32.
 * ``rmat``            R-MAT (a, b, c, d) = (0.57, 0.19, 0.19, 0.05), scale s,
-                      edge factor 16; self-loops and duplicates removed.
+                      edge factor 16; self-loops and duplicates removed;
+                      optionally with randomly permuted vertex ids.
 * ``grid``            n x n grid, 4-neighbour pairs; each pair is
                       bidirectional with p = 0.7, else one random
                       orientation; plus 0.1% x (grid arcs) uniform random
@@ -98,7 +99,10 @@ def planted_random(V: int = 1024, m: int = 8192, n_cycles: int = 16, lmin: int =
 
 
 def rmat(scale: int = 22, edge_factor: int = 16, a=0.57, b=0.19, c=0.19, seed: int = 1, device="cpu",
-         clean: bool = True) -> Tuple[int, torch.Tensor, torch.Tensor]:
+         clean: bool = True, permute: bool = False) -> Tuple[int, torch.Tensor, torch.Tensor]:
+    """R-MAT arcs.  With permute, vertex ids are relabelled by a seeded random
+    permutation (as Graph500 does), so that ids no longer follow degree: the
+    unpermuted generator gives the hubs the lowest ids."""
     V = 1 << scale
     m = edge_factor * V
     g = _gen(seed, device)
@@ -111,6 +115,9 @@ def rmat(scale: int = 22, edge_factor: int = 16, a=0.57, b=0.19, c=0.19, seed: i
         vb = (((r >= a) & (r < ab)) | (r >= abc)).to(torch.int64)  # quadrants b, d
         u |= ub << bit
         v |= vb << bit
+    if permute:
+        perm = torch.randperm(V, generator=_gen(seed + 7919, device), device=device)
+        u, v = perm[u], perm[v]
     u += 1
     v += 1
     if clean:

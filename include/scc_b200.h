@@ -163,11 +163,15 @@ const char *scc_version(void);
  * GPU that loads the library until the process exits); the caller passes
  * device CSR arrays (SCC_FLAG_DEVICE is required) and a device buffer of V
  * labels.  Graphs above SCC_NOALLOC_MAX_VERTICES / SCC_NOALLOC_MAX_EDGES
- * are rejected with SCC_ERR_TOO_LARGE.  The first call on a device (with
- * that device current) looks up the array's device address; make it before
- * any stream capture.  All calls share the array: calls that overlap on the
- * GPU race.  Calls no cudaMalloc, cudaFree or allocating library routine.
- * Synchronous; `stream` as in scc_run. */
+ * are rejected with SCC_ERR_TOO_LARGE.  Accepted flags: SCC_FLAG_DEVICE
+ * (required), SCC_FLAG_TRIM1, SCC_FLAG_TRIM2; any other flag is rejected with
+ * SCC_ERR_INVALID_ARG.  The first call on a device (with that device
+ * current) looks up the array's device address; make it before any stream
+ * capture.  The address is kept per CUDA context, so a call in a context
+ * created later (after cudaDeviceReset, say) looks it up again.  All calls
+ * share the array: calls that overlap on the GPU race.  Calls no cudaMalloc,
+ * cudaFree or allocating library routine.  Synchronous; `stream` as in
+ * scc_run. */
 #define SCC_NOALLOC_MAX_VERTICES 16384u
 #define SCC_NOALLOC_MAX_EDGES 262144u
 int scc_run_noalloc(const scc_csr_view *g, int algo, uint32_t flags, int warp_width, uint32_t *labels_out,

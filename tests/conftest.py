@@ -9,6 +9,8 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
+# reference checkout (read only), present in the build container only
+REFERENCE_DIR = os.environ.get("SCC_REFERENCE_DIR", "/root/reference")
 SAMPLES = ["sample0", "sample4", "sample5", "sample1", "sample128", "sample2"]
 
 

@@ -94,4 +94,4 @@ def main(data_dir: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/data")
+    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(os.environ.get("SCC_REFERENCE_DIR", "/root/reference"), "data"))

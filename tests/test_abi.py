@@ -6,7 +6,7 @@ import subprocess
 
 import pytest
 
-from conftest import ROOT
+from conftest import REFERENCE_DIR, ROOT
 
 
 def _declared_c_functions():
@@ -63,7 +63,7 @@ def test_reference_main_links_against_the_library(native, tmp_path):
     """The reference's own scc.cu (unchanged, compiled from the reference
     checkout where present) links against libscc_b200.so in place of its
     scc_kernels / scc_WCC / scc_Coloring / load objects."""
-    ref = "/root/reference"
+    ref = REFERENCE_DIR
     if not os.path.isdir(os.path.join(ref, "src")):
         pytest.skip("reference checkout not present")
     out = str(tmp_path / "scc_linked")

@@ -17,6 +17,7 @@ from conftest import ROOT, SAMPLES
 
 pytestmark = pytest.mark.gpu
 REF = os.path.join(ROOT, "oracle", "_ref", "scc_ref")
+LINKED = os.path.join(ROOT, "oracle", "_ref", "scc_linked")
 
 
 def _ref(path, algo, p, q, w):
@@ -108,3 +109,25 @@ def test_recorded_reference_counts(golden):
             assert r["num_sccs"] <= int(golden[name]["nscc"])
         else:
             assert r["num_sccs"] == int(golden[name]["nscc"]), key
+
+
+@pytest.mark.skipif(not os.path.exists(LINKED), reason="linked drop-in not built (make -C oracle linked)")
+@pytest.mark.parametrize("name", SAMPLES)
+@pytest.mark.parametrize("algo,p,q,w", [("g", 1, 0, 1), ("g", 1, 1, 1), ("x", 1, 0, 8), ("h", 1, 1, 1),
+                                        ("h", 0, 0, 1), ("y", 1, 1, 8), ("y", 0, 1, 4)])
+def test_reference_main_linked_against_the_library(native, golden, gr_files, name, algo, p, q, w):
+    """The reference's unchanged scc.cu linked against libscc_b200.so (its
+    vHong / vSlota / wHong / wSlota / loadFullGraph resolved from the
+    library) prints what this project's CLI prints and the SCC count of the
+    reference binary and of the fixture's known answer."""
+    args = ["-a", algo, "-p", str(p), "-q", str(q), "-w", str(w), "-f", gr_files[name]]
+    linked = subprocess.run([LINKED] + args, capture_output=True, text=True, timeout=120)
+    ours = _ours(native, gr_files[name], algo, p, q, w)
+    assert linked.returncode == 0 and ours.returncode == 0, (linked.stdout, linked.stderr)
+    norm = lambda s: re.sub(r"Time : [0-9.]+", "Time : T", s)  # noqa: E731
+    assert norm(linked.stdout) == norm(ours.stdout)
+    assert _count(linked.stdout, r"Number Of Sccs : (-?\d+)") == int(golden[name]["nscc"])
+    if os.path.exists(REF) and not (algo in "gx" and q == 1):   # the reference's Hong -q 1 can under-count
+        ref = _ref(gr_files[name], algo, p, q, w)
+        assert ref.returncode == 0
+        assert _count(ref.stdout, r"Number Of Sccs : (-?\d+)") == _count(linked.stdout, r"Number Of Sccs : (-?\d+)")

@@ -89,3 +89,52 @@ def test_noalloc_rejects_graphs_above_its_limit(native):
     small = _view(native, 3, E, Fr, Fc, Fr, Fc)
     rc = native.lib().scc_run_noalloc(ctypes.byref(small), ord("h"), 0, 1, out.data_ptr(), None, None)
     assert rc == 1  # SCC_ERR_INVALID_ARG
+
+
+def test_noalloc_at_its_exact_limit_matches_tarjan(native, oracle_lib):
+    """A graph of exactly SCC_NOALLOC_MAX_VERTICES vertices and
+    SCC_NOALLOC_MAX_EDGES arcs (duplicates kept) fits the built-in scratch
+    array: labels equal Tarjan's and scc_run's, twice in a row."""
+    import torch
+
+    import detectingscc_b200 as scc
+    V, E = 16384, 262144
+    rng = np.random.default_rng(17)
+    # uniform arcs, mean out-degree 16: one giant SCC plus trimmed vertices
+    src = rng.integers(1, V + 1, E)
+    dst = rng.integers(1, V + 1, E)
+    g = scc.graph_from_arcs(V, src, dst)
+    assert (g.V, g.E) == (V, E)
+    lab, n = oracle_lib.tarjan(g.V, g.Fr, g.Fc)
+    dev = [torch.from_numpy(a.view(np.int32)).cuda() for a in (g.Fr, g.Fc, g.Br, g.Bc)]
+    stream = torch.cuda.current_stream().cuda_stream
+    view = _view(native, V, E, *dev)
+    eng = scc.Engine(0)
+    try:
+        ref = torch.empty(V, dtype=torch.int32, device="cuda")
+        r = eng.run_device(V, E, *dev, labels_out=ref, algo="h")
+    finally:
+        eng.close()
+    assert r.num_sccs == n
+    for algo in ("h", "g"):
+        for _ in range(2):
+            out = torch.full((V,), -1, dtype=torch.int32, device="cuda")
+            rc, st = _noalloc(native, view, algo, native.FLAG_TRIM1 | native.FLAG_TRIM2, 1, out, stream)
+            assert rc == 0, native.status_string(rc)
+            assert st.num_sccs == n
+            got = out.cpu().numpy().view(np.uint32)
+            assert np.array_equal(got, lab[1:])
+            if algo == "h":
+                assert torch.equal(out, ref)
+
+
+def test_noalloc_rejects_flags_it_does_not_use(native):
+    import torch
+    V, E = 4, 2
+    Fr = torch.tensor([0, 0, 1, 2, 2, 2], dtype=torch.int32, device="cuda")
+    Fc = torch.tensor([2, 3], dtype=torch.int32, device="cuda")
+    out = torch.empty(V, dtype=torch.int32, device="cuda")
+    view = _view(native, V, E, Fr, Fc, Fr, Fc)
+    for extra in (native.FLAG_DERIVE_REVERSE, native.FLAG_FORCE_GRID, native.FLAG_INSTRUMENT):
+        rc, _ = _noalloc(native, view, "h", extra, 1, out, None)
+        assert rc == 1  # SCC_ERR_INVALID_ARG
