@@ -104,7 +104,8 @@ class Engine:
 
     PHASES = {1: "init", 2: "trim1_once", 3: "trim1_apply", 4: "trim1_fix", 5: "trim2", 6: "trim2_apply",
               7: "first_pivot", 8: "bfs0", 9: "bfs", 10: "prop", 11: "hong_update", 12: "slota_first_update",
-              13: "slota_peel_update", 14: "rename", 15: "pivots", 16: "bfs_pull", 17: "prop_pull"}
+              13: "slota_peel_update", 14: "rename", 15: "pivots", 16: "bfs_pull", 17: "prop_pull",
+              18: "res_tag", 19: "res_extract", 20: "res_solve"}
 
     def trace(self):
         """Per-pass (phase, microseconds, items pushed) of the last run (needs set_tuning('trace', n))."""
@@ -357,14 +358,32 @@ def save_binary(path: str, g: Graph) -> None:
     N.check(N.lib().scc_save_binary(path.encode(), ctypes.byref(hg)), f"save {path}")
 
 
+def save_metis(path: str, g: Graph) -> None:
+    """Write g in the reference converter's METIS input layout (MetisInput.cpp:114-131)."""
+    hg = N.HostGraph(g.V, g.E, g.Fr.ctypes.data_as(N.u32p), g.Fc.ctypes.data_as(N.u32p),
+                     g.Br.ctypes.data_as(N.u32p), g.Bc.ctypes.data_as(N.u32p), None)
+    N.check(N.lib().scc_save_metis(path.encode(), ctypes.byref(hg)), f"save {path}")
+
+
+def load_partition(path: str, V: int) -> np.ndarray:
+    """METIS partition ids as Pr[0..V+1] (Pr[v] for vertex v; load.cpp:115-130)."""
+    Pr = np.zeros(V + 2, dtype=np.uint32)
+    N.check(N.lib().scc_load_partition(path.encode(), int(V), _ptr(Pr)), f"load {path}")
+    return Pr
+
+
 def loadFullGraph(filename: str):
     """The reference's loader: returns (CSize, RSize, Fc, Fr, Bc, Br, Pr).
 
-    Pr (METIS partition ids, read only by the reference's detectSCC) is
-    zero-filled.
+    Pr (METIS partition ids, read only by the reference's detectSCC) comes
+    from the file named by SCC_METIS_PARTITION when it is set (the
+    reference reads a fixed path, load.cpp:115-130), else it is zero-filled.
     """
+    import os
     g = load_graph(filename)
-    return g.E, g.V, g.Fc, g.Fr, g.Bc, g.Br, np.zeros(g.V + 2, dtype=np.uint32)
+    part = os.environ.get("SCC_METIS_PARTITION")
+    Pr = load_partition(part, g.V) if part else np.zeros(g.V + 2, dtype=np.uint32)
+    return g.E, g.V, g.Fc, g.Fr, g.Bc, g.Br, Pr
 
 
 # ----------------------------------------------------------------------

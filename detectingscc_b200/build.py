@@ -7,6 +7,7 @@ Produces
                                        reference-signature shims
                                        (include/scc_compat.h)
     detectingscc_b200/bin/scc          the drop-in command line
+    detectingscc_b200/bin/scc_metis    the METIS input converter (MetisInput.cpp)
 
 CUDA code is compiled for sm_100a only; the CUDA runtime is linked
 statically so the library does not depend on which libcudart a host
@@ -25,6 +26,7 @@ CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libscc_b200.so")
 CLI = os.path.join(PKG, "bin", "scc")
+CLI_METIS = os.path.join(PKG, "bin", "scc_metis")
 
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -33,7 +35,7 @@ CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-Wall", "-I/usr/local/cuda/include"]
 
 CU_SOURCES = ["scc_engine.cu", "scc_batch.cu", "scc_noalloc.cu", "scc_serve.cu", "scc_transpose.cu"]
 CXX_LIB_SOURCES = ["gtgraph_load.cpp", "scc_compat.cpp"]
-CXX_CLI_SOURCES = ["scc_cli.cpp"]
+CXX_CLI_SOURCES = ["scc_cli.cpp", "scc_metis_cli.cpp"]
 HEADERS = ["scc_device.cuh", "scc_phases.cuh", "scc_internal.h", "scc_host.h", "scc_batch_internal.h"]
 
 
@@ -79,9 +81,10 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> str:
     all_lib = objs + lib_objs
     if force or _newer(LIB, all_lib):
         _run([NVCC] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-o", LIB] + all_lib + ["-lpthread"])
-    cli_obj = os.path.join(BUILD, "scc_cli.cpp.o")
-    if force or _newer(CLI, all_lib + [cli_obj]):
-        _run([NVCC] + ARCH + ["-o", CLI, cli_obj] + all_lib + ["-lpthread"])
+    for exe, src in ((CLI, "scc_cli.cpp"), (CLI_METIS, "scc_metis_cli.cpp")):
+        cli_obj = os.path.join(BUILD, src + ".o")
+        if force or _newer(exe, all_lib + [cli_obj]):
+            _run([NVCC] + ARCH + ["-o", exe, cli_obj] + all_lib + ["-lpthread"])
     return LIB
 
 

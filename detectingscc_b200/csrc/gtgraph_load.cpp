@@ -11,9 +11,9 @@
 // Differences: the (u, v) order comes from two stable counting sorts
 // (O(E + V)) instead of std::sort; ids outside [1, V] and short files are
 // reported instead of being undefined behaviour; the METIS partition array
-// Pr, which only the out-of-scope detectSCC driver reads, is zero-filled
-// instead of being read from the reference's hardcoded path
-// (load.cpp:115-130).  Files that start with "SCCBIN01" are read as the
+// Pr, which only the detectSCC driver reads, is read from the file named by
+// SCC_METIS_PARTITION (zero-filled without it) instead of the reference's
+// hardcoded path (load.cpp:115-130).  Files that start with "SCCBIN01" are read as the
 // project's binary CSR (see scc_load_graph).
 #include <cstdint>
 #include <cstdio>
@@ -215,6 +215,84 @@ extern "C" int scc_save_binary(const char *path, const scc_host_graph *g)
     return ok ? SCC_OK : SCC_ERR_IO;
 }
 
+namespace {
+
+// Appends the decimal digits of x and one space.
+inline char *put_u32_sp(char *o, uint32_t x)
+{
+    char tmp[10];
+    int n = 0;
+    do {
+        tmp[n++] = (char)('0' + x % 10u);
+        x /= 10u;
+    } while (x);
+    while (n) *o++ = tmp[--n];
+    *o++ = ' ';
+    return o;
+}
+
+}  // namespace
+
+// The reference converter's METIS layout (MetisInput.cpp:114-131): "V E",
+// then per vertex its forward list and its reverse list.  Written through
+// one buffer flushed every few MB.
+extern "C" int scc_save_metis(const char *path, const scc_host_graph *g)
+{
+    if (!path || !g || (g->V && (!g->Fr || !g->Br)) || (g->E && (!g->Fc || !g->Bc))) return SCC_ERR_INVALID_ARG;
+    FILE *f = fopen(path, "wb");
+    if (!f) return SCC_ERR_IO;
+    const size_t cap = 4u << 20;
+    std::vector<char> buf;
+    try {
+        buf.resize(cap + 64);
+    } catch (...) {
+        fclose(f);
+        return SCC_ERR_OOM;
+    }
+    char *o = buf.data();
+    bool ok = true;
+    auto flush = [&](bool force) {
+        if (force || (size_t)(o - buf.data()) >= cap) {
+            const size_t n = (size_t)(o - buf.data());
+            ok = ok && fwrite(buf.data(), 1, n, f) == n;
+            o = buf.data();
+        }
+    };
+    o += snprintf(o, 64, "%u %u\n", g->V, g->E);
+    for (uint32_t v = 1; v <= g->V; v++) {
+        for (uint32_t e = g->Fr[v]; e < g->Fr[v + 1]; e++) {
+            o = put_u32_sp(o, g->Fc[e]);
+            flush(false);
+        }
+        for (uint32_t e = g->Br[v]; e < g->Br[v + 1]; e++) {
+            o = put_u32_sp(o, g->Bc[e]);
+            flush(false);
+        }
+        *o++ = '\n';
+        flush(false);
+    }
+    flush(true);
+    ok = (fclose(f) == 0) && ok;
+    return ok ? SCC_OK : SCC_ERR_IO;
+}
+
+// One partition id per vertex, whitespace separated (load.cpp:127-131).
+extern "C" int scc_load_partition(const char *path, uint32_t V, uint32_t *Pr)
+{
+    if (!path || !Pr) return SCC_ERR_INVALID_ARG;
+    Buf b;
+    if (!read_file(path, b)) return SCC_ERR_IO;
+    const char *s = b.p, *e = b.p + b.n;
+    Pr[0] = 0;
+    Pr[V + 1] = 0;
+    for (uint32_t k = 1; k <= V; k++) {
+        uint64_t x = 0;
+        if (!read_u64(s, e, x) || x > 0xFFFFFFFFull) return SCC_ERR_BAD_GRAPH;
+        Pr[k] = (uint32_t)x;
+    }
+    return SCC_OK;
+}
+
 // The reference's loader signature (load.h:6).  On a read failure it prints
 // the reference's message and leaves empty outputs (the reference returns
 // with them unset, load.cpp:24-28).
@@ -226,6 +304,18 @@ void loadFullGraph(const char *filename, uint32_t *oCSize, uint32_t *oRSize, uin
     if (rc != SCC_OK) {
         if (rc == SCC_ERR_IO) printf("Error Reading graph file\n");
         else fprintf(stderr, "loadFullGraph: %s: %s\n", filename, scc_status_string(rc));
+        *oCSize = 0;
+        *oRSize = 0;
+        *oFc = *oFr = *oBc = *oBr = *oPr = nullptr;
+        return;
+    }
+    // the METIS partition that only detectSCC reads: the reference opens a
+    // fixed path (load.cpp:115-130); here the path comes from the
+    // environment, and its absence leaves Pr zero-filled (one partition)
+    const char *part = getenv("SCC_METIS_PARTITION");
+    if (part && *part && g.Pr && scc_load_partition(part, g.V, g.Pr) != SCC_OK) {
+        printf("Error Reading metis graph file\n");
+        scc_free_host_graph(&g);
         *oCSize = 0;
         *oRSize = 0;
         *oFc = *oFr = *oBc = *oBr = *oPr = nullptr;

@@ -83,7 +83,7 @@ __device__ void batch_one(Ex &ex, const BatchParams &p, uint32_t gi, char *base,
         uint32_t *o = p.out + bg.off_out;
         for (uint32_t v = ex.tid() + 1u; v <= bg.V; v += ex.nthr()) {
             const uint32_t l = w.label[v];
-            o[v - 1u] = l <= bg.V ? w.smin[l] : 0u;
+            o[v - 1u] = (l & LBL_SELF) ? (l & ~LBL_SELF) : (l <= bg.V ? w.smin[l] : 0u);
         }
     }
     if (ex.leader())
@@ -152,7 +152,8 @@ void *pick_batch_kernel(int threads, bool hong, bool cl = false)
     }
 }
 
-size_t batch_smem(int threads, uint32_t qcap) { return (BQ_HDR + NBQ * (size_t)(threads / 32) * qcap) * 4; }
+// two staging queues per CTA (the batched graphs run on single CTAs and clusters)
+size_t batch_smem(int threads, uint32_t qcap) { return (BQ_HDR + 2 * (size_t)(threads / 32) * qcap) * 4; }
 
 }  // namespace
 

@@ -28,6 +28,10 @@ constexpr uint32_t FVB = 0x40000000u;
 constexpr uint32_t BVB = 0x80000000u;
 constexpr uint32_t FULL = 0xFFFFFFFFu;
 constexpr uint32_t MAX_V = 0x0FFFFFFEu;   // 4V+3 split names must stay below DEAD
+// label[v] with this bit set holds v's canonical label itself (the low
+// bits): a vertex that is its own SCC (trim-1, trim-2, small residual SCCs)
+// needs no smin entry and no gather when the labels are written out.
+constexpr uint32_t LBL_SELF = 0x80000000u;
 
 // Load-balancing constants of the frontier expansion: a frontier vertex
 // whose degree exceeds HEAVY_T is cut into CH-edge chunks that the next pass
@@ -41,7 +45,7 @@ constexpr int E_NOT_CONVERGED = 21;
 constexpr int E_TIMEOUT = 22;
 constexpr int E_BAD_GRAPH = 23;
 
-enum { C_FQ = 0, C_BQ = 1, C_FH = 2, C_BH = 3, C_LIST = 4, C_FE = 5, C_BE = 6, C_RNG = 7, NCNT = 8 };
+enum { C_FQ = 0, C_BQ = 1, C_FH = 2, C_BH = 3, C_LIST = 4, C_FE = 5, C_BE = 6, C_RNG = 7, C_SCOPE = 8, NCNT = 9 };
 
 struct __align__(128) Ctl {
     // grid barrier arrival counter and the sticky error code share one
@@ -49,7 +53,7 @@ struct __align__(128) Ctl {
     unsigned bar_count;
     int error;
     int where; unsigned _p0[29];
-    unsigned lc[3][NCNT]; unsigned _p3[8];         // per-pass counters, 3-slot ring
+    unsigned lc[3][NCNT]; unsigned _p3[5];         // per-pass counters, 3-slot ring
     unsigned long long n_trim1, n_trim2, n_pivot;
     unsigned long long t_edges, t_verts;           // instrumented work counters
     unsigned passes, outer;                        // passes run, peels / iterations
@@ -66,7 +70,8 @@ struct __align__(128) Ctl {
 enum {
     PH_INIT = 1, PH_TRIM1_ONCE = 2, PH_TRIM1_APPLY = 3, PH_TRIM1_FIX = 4, PH_TRIM2 = 5, PH_TRIM2_APPLY = 6,
     PH_FIRST_PIVOT = 7, PH_BFS0 = 8, PH_BFS = 9, PH_PROP = 10, PH_HONG_UPDATE = 11, PH_SLOTA_FIRST_UPDATE = 12,
-    PH_SLOTA_PEEL_UPDATE = 13, PH_RENAME = 14, PH_PIVOTS = 15, PH_BFS_PULL = 16, PH_PROP_PULL = 17
+    PH_SLOTA_PEEL_UPDATE = 13, PH_RENAME = 14, PH_PIVOTS = 15, PH_BFS_PULL = 16, PH_PROP_PULL = 17,
+    PH_RES_TAG = 18, PH_RES_EXTRACT = 19, PH_RES_SOLVE = 20
 };
 
 struct Graph {
@@ -93,7 +98,8 @@ __device__ __forceinline__ void load_off5(const uint32_t *__restrict__ R, uint32
 
 struct Work {
     uint32_t *st, *label, *stamp;
-    uint32_t *smin;             // smin[r] = smallest member id of the SCC represented by r
+    uint32_t *smin;             // smin[r] = smallest member id of the SCC represented by r; set to r
+                                // when r becomes a representative (its seed pass), then folded
     uint32_t *L[2];
     uint32_t *Q[2][2];          // [direction][parity]
     uint2 *H[2][2];             // heavy chunks (vertex, chunk) [direction][parity]
@@ -138,10 +144,12 @@ __host__ __device__ inline size_t carve_work(char *base, uint32_t V, uint32_t E,
     return 10 * va + 4 * ha + pa + ca;
 }
 
-// Dynamic shared memory of the SCC kernels: BQ_HDR control words, then NBQ
-// staging queues, each split into one slice of qcap entries per warp of the
-// CTA: (BQ_HDR + NBQ * warps * qcap) words.
-constexpr unsigned NBQ = 2;
+// Dynamic shared memory of the SCC kernels: BQ_HDR control words, then the
+// staging queues (at most NBQ: two frontier queues, and on the whole-GPU
+// kernel a third one for the shrinking bottom-up scope), each split into
+// one slice of qcap entries per warp of the CTA: (BQ_HDR + queues * warps *
+// qcap) words.
+constexpr unsigned NBQ = 3;
 constexpr unsigned BQ_WARPS = 32;                       // at most 1024 threads per CTA
 constexpr unsigned BQ_CNT = 16;                         // per-warp fill counts [NBQ][BQ_WARPS]
 constexpr unsigned BQ_PRE = BQ_CNT + NBQ * BQ_WARPS;    // per-warp flush offsets [NBQ][BQ_WARPS]
@@ -196,6 +204,8 @@ template <bool INSTR>
 struct GridExec {
     static constexpr bool instr = INSTR;
     static constexpr bool grid = true;
+    static constexpr bool cluster = false;
+    static constexpr unsigned nbq = 3;   // staging queues of the launch's shared memory
     Ctl *ctl;
     unsigned gl;        // pass counter, identical in every thread
     unsigned cap = 0;   // pass cap of the run (0: none), see run_pass
@@ -257,6 +267,8 @@ template <bool INSTR>
 struct BlockExec {
     static constexpr bool instr = INSTR;
     static constexpr bool grid = false;
+    static constexpr bool cluster = false;
+    static constexpr unsigned nbq = 2;
     Ctl *ctl;
     unsigned gl;
     unsigned cap = 0;
@@ -312,6 +324,8 @@ template <bool INSTR>
 struct ClusterExec {
     static constexpr bool instr = INSTR;
     static constexpr bool grid = false;
+    static constexpr bool cluster = true;
+    static constexpr unsigned nbq = 2;
     Ctl *ctl;
     unsigned gl;
     unsigned rank, csize;
@@ -485,7 +499,7 @@ __device__ __forceinline__ void bq_add_edges(unsigned qi, unsigned x)
 // (optional) receive the CTA's frontier-edge tallies.
 __device__ __forceinline__ void bq_flush(unsigned nq, uint32_t qcap, uint32_t *gq0, unsigned *gcnt0, uint32_t *gq1,
                                          unsigned *gcnt1, uint32_t gcap, Ctl *ctl, unsigned *ecnt0 = nullptr,
-                                         unsigned *ecnt1 = nullptr)
+                                         unsigned *ecnt1 = nullptr, uint32_t *gq2 = nullptr, unsigned *gcnt2 = nullptr)
 {
     __syncthreads();
     const unsigned nw = blockDim.x >> 5;
@@ -496,8 +510,8 @@ __device__ __forceinline__ void bq_flush(unsigned nq, uint32_t qcap, uint32_t *g
                 sccb_dsmem[BQ_PRE + qi * BQ_WARPS + wi] = total;
                 total += sccb_dsmem[BQ_CNT + qi * BQ_WARPS + wi];
             }
-            sccb_dsmem[8 + qi] = total ? atomicAdd(qi ? gcnt1 : gcnt0, total) : 0u;
-            unsigned *ec = qi ? ecnt1 : ecnt0;
+            sccb_dsmem[8 + qi] = total ? atomicAdd(qi == 2 ? gcnt2 : qi ? gcnt1 : gcnt0, total) : 0u;
+            unsigned *ec = qi == 2 ? nullptr : qi ? ecnt1 : ecnt0;
             if (ec && sccb_dsmem[12 + qi]) atomicAdd(ec, sccb_dsmem[12 + qi]);
             sccb_dsmem[12 + qi] = 0u;
         }
@@ -505,7 +519,7 @@ __device__ __forceinline__ void bq_flush(unsigned nq, uint32_t qcap, uint32_t *g
     __syncthreads();
     const unsigned wi = threadIdx.x >> 5;
     for (unsigned qi = 0; qi < nq; qi++) {
-        uint32_t *gq = qi ? gq1 : gq0;
+        uint32_t *gq = qi == 2 ? gq2 : qi ? gq1 : gq0;
         const unsigned cnt = sccb_dsmem[BQ_CNT + qi * BQ_WARPS + wi];
         const unsigned base = sccb_dsmem[8 + qi] + sccb_dsmem[BQ_PRE + qi * BQ_WARPS + wi];
         const uint32_t *slice = &sccb_dsmem[BQ_HDR + (qi * nw + wi) * qcap];
@@ -515,6 +529,18 @@ __device__ __forceinline__ void bq_flush(unsigned nq, uint32_t qcap, uint32_t *g
         }
         __syncwarp();
         if (lane_id() == 0) sccb_dsmem[BQ_CNT + qi * BQ_WARPS + wi] = 0u;
+    }
+}
+
+// Adds the CTA's frontier-edge tally of queue 0 (word 12) to *ecnt and
+// clears it: the end of a pass that tallies without staging queues.
+// Called by every thread of the CTA.
+__device__ __forceinline__ void bq_flush_edges(unsigned *ecnt)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (sccb_dsmem[12]) atomicAdd(ecnt, sccb_dsmem[12]);
+        sccb_dsmem[12] = 0u;
     }
 }
 

@@ -35,7 +35,7 @@ struct Params {
 
 // Canonical labels of vertices tid+1, tid+1+n, ...: every vertex takes the
 // smallest member id of its SCC, which the update passes fold into
-// smin[representative].  Runs after the last pass barrier, so label and
+// smin[representative] (or label[v] holds it itself, LBL_SELF).  Runs after the last pass barrier, so label and
 // smin are final.  Four vertices per thread and round: their label loads,
 // then their smin gathers, are issued back to back, so a thread waits on
 // two memory latencies per four vertices instead of two per vertex.  The
@@ -55,7 +55,8 @@ __device__ __forceinline__ void canon_labels(const uint32_t *label, const uint32
             l[j] = v <= V ? label[v] : 0xFFFFFFFFu;
         }
 #pragma unroll
-        for (uint32_t j = 0; j < LABEL_UNROLL; ++j) l[j] = l[j] <= V ? smin[l[j]] : 0u;
+        for (uint32_t j = 0; j < LABEL_UNROLL; ++j)
+            l[j] = (l[j] & LBL_SELF) ? (l[j] & ~LBL_SELF) : (l[j] <= V ? smin[l[j]] : 0u);
 #pragma unroll
         for (uint32_t j = 0; j < LABEL_UNROLL; ++j) {
             const uint32_t v = v0 + j * n;
@@ -75,9 +76,10 @@ __device__ __forceinline__ void write_labels(const Work &w, uint32_t V, uint32_t
 constexpr int GRID_THREADS = 1024;
 constexpr int BLOCK_THREADS = 1024;
 
-static size_t dyn_smem_bytes(uint32_t qcap, int threads = 1024)
+// queues: staging queues of the launch (3 on the whole-GPU kernel, 2 on one CTA)
+static size_t dyn_smem_bytes(uint32_t qcap, unsigned queues, int threads = 1024)
 {
-    return (BQ_HDR + NBQ * (size_t)(threads / 32) * qcap) * sizeof(uint32_t);
+    return (BQ_HDR + queues * (size_t)(threads / 32) * qcap) * sizeof(uint32_t);
 }
 
 template <bool INSTR, bool HONG>
@@ -90,6 +92,14 @@ __global__ void __launch_bounds__(GRID_THREADS, 1) k_scc_grid(Params p)
     Carry cy{0u, 0u, 0u};
     int rc = HONG ? hong_front(ex, p.g, p.w, p.t1, p.t2, p.lw, cy) : slota_front(ex, p.g, p.w, p.t1, p.lw, cy);
     if (rc == RUN_DONE) rc = HONG ? hong_loop(ex, p.g, p.w, cy, p.tail_n) : slota_peels(ex, p.g, p.w, cy, p.tail_n);
+    if (rc == RUN_RESIDUAL) {
+        // the live vertices fit one CTA's shared memory: CTA 0 solves them
+        if (blockIdx.x != 0) return;
+        res_solve(p.g, p.w, p.w.L[cy.lsel], cy.nL, p.w.Q[1][(cy.gl - 1u) & 1u], last_count(ex, C_BQ), p.w.ctl);
+        res_trace(p.w.ctl, cy.gl, cy.nL);
+        if (threadIdx.x == 0) { p.w.ctl->tail_pass = cy.gl; p.w.ctl->nlive_tail = cy.nL; p.w.ctl->passes = cy.gl + 1u; }
+        return;
+    }
     if (rc == RUN_SWITCH) {
         // the live set is small: CTA 0 finishes alone with block barriers
         if (blockIdx.x != 0) return;
@@ -97,6 +107,7 @@ __global__ void __launch_bounds__(GRID_THREADS, 1) k_scc_grid(Params p)
         BlockExec<INSTR> bx{p.w.ctl, cy.gl, p.pass_cap};
         if (HONG) hong_loop(bx, p.g, p.w, cy, 0u);
         else slota_peels(bx, p.g, p.w, cy, 0u);
+        bx.gl = cy.gl;
         if (threadIdx.x == 0) p.w.ctl->passes = bx.gl;
         return;
     }
@@ -360,8 +371,8 @@ int sccb_smem_limit(void *fn, size_t max_bytes)
 }
 
 // Largest dynamic shared memory of the plain-path kernels: the staging
-// slice is at most 768 entries (scc_set_tuning "qcap").
-static size_t max_plain_smem() { return dyn_smem_bytes(768); }
+// slice is at most 576 entries (scc_set_tuning "qcap") in three queues.
+static size_t max_plain_smem() { return dyn_smem_bytes(576, 3); }
 
 // Makes sure the kernel's dynamic shared memory limit covers every launch
 // of it and returns the grid of its cooperative launch, computed once per
@@ -462,7 +473,7 @@ extern "C" int scc_run(scc_context *ctx, const scc_csr_view *gv, int algo, uint3
 
     ctx->work.qcap = ctx->qcap;
     ctx->work.bu_k = ctx->bu_k;
-    const size_t smem = dyn_smem_bytes(ctx->qcap);
+    const size_t smem_block = dyn_smem_bytes(ctx->qcap, 2), smem_grid = dyn_smem_bytes(ctx->qcap, 3);
     Params p{g, ctx->work, (flags & SCC_FLAG_TRIM1) ? 1 : 0, (flags & SCC_FLAG_TRIM2) ? 1 : 0, lw, ctx->tail_vertices,
              dout, ctx->max_passes, ctx->hold_pass};
     bool use_block = (V <= ctx->block_max_vertices && E <= ctx->block_max_edges);
@@ -473,15 +484,15 @@ extern "C" int scc_run(scc_context *ctx, const scc_csr_view *gv, int algo, uint3
     CK(cudaEventRecord(ctx->ev[1], st));
     if (use_block) {
         void *fn = pick_block(instr, hong);
-        if (prepare_kernel(ctx, fn, smem, BLOCK_THREADS) <= 0) return SCC_ERR_CUDA;
+        if (prepare_kernel(ctx, fn, smem_block, BLOCK_THREADS) <= 0) return SCC_ERR_CUDA;
         void *args[] = {&p};
-        CK(cudaLaunchKernel(fn, dim3(1), dim3(BLOCK_THREADS), args, smem, st));
+        CK(cudaLaunchKernel(fn, dim3(1), dim3(BLOCK_THREADS), args, smem_block, st));
     } else {
         void *fn = pick_grid(instr, hong);
-        nblocks = prepare_kernel(ctx, fn, smem, GRID_THREADS);
+        nblocks = prepare_kernel(ctx, fn, smem_grid, GRID_THREADS);
         if (nblocks <= 0) return SCC_ERR_CUDA;
         void *args[] = {&p};
-        CK(cudaLaunchCooperativeKernel(fn, dim3(nblocks), dim3(GRID_THREADS), args, smem, st));
+        CK(cudaLaunchCooperativeKernel(fn, dim3(nblocks), dim3(GRID_THREADS), args, smem_grid, st));
     }
     launches++;
     CK(cudaEventRecord(ctx->ev[2], st));
@@ -530,7 +541,7 @@ extern "C" int scc_set_tuning(scc_context *ctx, const char *key, long long value
     else if (!strcmp(key, "max_passes")) ctx->max_passes = (uint32_t)value;
     else if (!strcmp(key, "test_withhold_arrival")) ctx->hold_pass = (uint32_t)value;
     else if (!strcmp(key, "qcap")) {
-        if (value < 32 || value > 768) return SCC_ERR_INVALID_ARG;
+        if (value < 32 || value > 576) return SCC_ERR_INVALID_ARG;
         ctx->qcap = (uint32_t)value;
     } else if (!strcmp(key, "trace")) {
         // per-pass trace of the next runs: `value` passes (0 switches it off)
@@ -570,7 +581,7 @@ extern "C" int scc_get_trace(scc_context *ctx, uint64_t *out, uint32_t cap, uint
 int sccb_launch_block_path(const Graph &g, const Work &w, int t1, int t2, int lw, bool hong, uint32_t *dout,
                            cudaStream_t st, unsigned *launches)
 {
-    const size_t smem = dyn_smem_bytes(w.qcap);
+    const size_t smem = dyn_smem_bytes(w.qcap, 2);
     void *fn = pick_block(false, hong);
     if (smem > max_plain_smem()) return SCC_ERR_INVALID_ARG;
     const int rc = sccb_smem_limit(fn, max_plain_smem());

@@ -153,12 +153,10 @@ __device__ bool ph_init(Ex &ex, const Graph &g, const Work &w, bool fold_pivot)
             if (i0 + 3u <= g.V) {
                 *reinterpret_cast<uint4 *>(w.st + i0) = make_uint4(i0 == 0u ? DEAD : 0u, 0u, 0u, 0u);
                 *reinterpret_cast<uint4 *>(w.stamp + i0) = make_uint4(0u, 0u, 0u, 0u);
-                *reinterpret_cast<uint4 *>(w.smin + i0) = make_uint4(DEAD, DEAD, DEAD, DEAD);
             } else {
                 for (uint32_t i = i0; i <= g.V; i++) {
                     w.st[i] = (i == 0u) ? DEAD : 0u;
                     w.stamp[i] = 0u;
-                    w.smin[i] = DEAD;
                 }
             }
         }
@@ -171,9 +169,13 @@ __device__ bool ph_init(Ex &ex, const Graph &g, const Work &w, bool fold_pivot)
 // init and trim1-once in one sweep (vSlota / wSlota with trim1): with every
 // vertex live in range 0, trim1 is decided by the degrees alone, so the
 // offsets the init pass validates also decide each vertex's first state.
-// Four ids per lane: 128-bit offset loads and 128-bit stores of st, stamp,
-// smin and label.  Survivors are compacted into Lout and bid for the first
-// pivot.  A bad graph sets the error before the barrier, as in ph_init.
+// Four ids per lane: 128-bit offset loads and 128-bit stores of st and
+// label (a trimmed vertex is labelled with itself, LBL_SELF).  Stamps are
+// cleared later for the few vertices that need them (ph_slota_first_update)
+// and smin entries when their representative is seeded, so this sweep
+// writes two vertex arrays, not four.  Survivors are compacted into Lout and
+// bid for the first pivot.  A bad graph sets the error before the barrier,
+// as in ph_init.
 // ---------------------------------------------------------------------
 template <class Ex>
 __device__ bool ph_init_trim1(Ex &ex, const Graph &g, const Work &w, uint32_t *Lout)
@@ -195,20 +197,19 @@ __device__ bool ph_init_trim1(Ex &ex, const Graph &g, const Work &w, uint32_t *L
 #pragma unroll
                 for (int j = 0; j < 5; j++) f[j] = b[j] = 0u;
             }
-            uint32_t st4[4], sm4[4], lb4[4];
+            uint32_t st4[4], lb4[4];
 #pragma unroll
             for (int j = 0; j < 4; j++) {
                 const uint32_t v = i0 + (uint32_t)j;
                 const bool valid = v >= 1u && v <= g.V;
                 bool surv = false;
                 st4[j] = DEAD;
-                sm4[j] = DEAD;
                 lb4[j] = v;
                 if (v <= g.V) bad |= f[j] > f[j + 1] || b[j] > b[j + 1];
                 if (valid) {
                     const uint32_t indeg = b[j + 1] - b[j], outdeg = f[j + 1] - f[j];
                     if (indeg == 0u || outdeg == 0u) {
-                        sm4[j] = v;      // a trimmed vertex is its own SCC
+                        lb4[j] = v | LBL_SELF;   // a trimmed vertex is its own SCC
                         ntrim++;
                     } else {
                         surv = true;
@@ -221,8 +222,6 @@ __device__ bool ph_init_trim1(Ex &ex, const Graph &g, const Work &w, uint32_t *L
             }
             if (i0 + 3u <= g.V) {
                 *reinterpret_cast<uint4 *>(w.st + i0) = make_uint4(st4[0], st4[1], st4[2], st4[3]);
-                *reinterpret_cast<uint4 *>(w.stamp + i0) = make_uint4(0u, 0u, 0u, 0u);
-                *reinterpret_cast<uint4 *>(w.smin + i0) = make_uint4(sm4[0], sm4[1], sm4[2], sm4[3]);
                 *reinterpret_cast<uint4 *>(w.label + i0) = make_uint4(lb4[0], lb4[1], lb4[2], lb4[3]);
             } else {
 #pragma unroll
@@ -230,8 +229,6 @@ __device__ bool ph_init_trim1(Ex &ex, const Graph &g, const Work &w, uint32_t *L
                     const uint32_t i = i0 + (uint32_t)j;
                     if (i <= g.V) {
                         w.st[i] = st4[j];
-                        w.stamp[i] = 0u;
-                        w.smin[i] = sm4[j];
                         w.label[i] = lb4[j];
                     }
                 }
@@ -276,7 +273,7 @@ __device__ bool ph_trim1_fix(Ex &ex, const Graph &g, const Work &w, VList src0, 
                         else
                             trim = !has_live(ex, w.st, g.Br, g.Bc, v, r, g.V) ||
                                    !has_live(ex, w.st, g.Fr, g.Fc, v, r, g.V);
-                        if (trim) { w.st[v] = DEAD; w.label[v] = v; w.smin[v] = v; }
+                        if (trim) { w.st[v] = DEAD; w.label[v] = v | LBL_SELF; }
                     }
                 }
                 count_verts(ex, valid);
@@ -334,8 +331,7 @@ __device__ bool ph_trim2(Ex &ex, const Graph &g, const Work &w, VList src)
                     if (k) {
                         hit = true;
                         cnt = v <= k;
-                        w.label[v] = v < k ? v : k;
-                        if (v <= k) w.smin[v] = v;
+                        w.label[v] = (v < k ? v : k) | LBL_SELF;
                     }
                 }
             }
@@ -491,9 +487,14 @@ __device__ __forceinline__ void chunk_expand(Ex &ex, const uint32_t *__restrict_
 // the rest by the whole warp.  A live vertex outside the scope can only
 // find a visited neighbour of its own range if its range is being
 // searched, so walking ids reaches the same set as walking the scope.
+//
+// With sout set (whole-GPU policy, first bottom-up step of a search), every
+// live vertex of the item that is still unvisited in a direction of the
+// search is appended to sout (staging queue 2): the scope of the next
+// bottom-up step, which then walks only those instead of the whole scope.
 template <class Ex>
-__device__ __forceinline__ void bfs_pull2(Ex &ex, const Graph &g, const Work &w, bool puf, bool pub, VList src,
-                                          uint32_t k, unsigned par, unsigned nxt)
+__device__ __forceinline__ void bfs_pull2(Ex &ex, const Graph &g, const Work &w, bool puf, bool pub, bool bw,
+                                          VList src, uint32_t k, unsigned par, unsigned nxt, uint32_t *sout)
 {
     constexpr uint32_t MF = RMASK | FVB, MB = RMASK | BVB;
     uint32_t v[2], s[2], pos[4], end[4], want[4];
@@ -584,6 +585,11 @@ __device__ __forceinline__ void bfs_pull2(Ex &ex, const Graph &g, const Work &w,
         count_verts(ex, ok[h]);
         if (puf) bq_push(0u, found[2 * h], v[h], w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_FQ], g.V, ex.ctl, 19);
         if (pub) bq_push(1u, found[2 * h + 1], v[h], w.qcap, w.Q[1][par], &ex.ctl->lc[nxt][C_BQ], g.V, ex.ctl, 19);
+        if (Ex::nbq > 2 && sout) {
+            const bool fv = (s[h] & FVB) || found[2 * h], bv = (s[h] & BVB) || found[2 * h + 1];
+            const bool keep = s[h] != DEAD && !(fv && (bv || !bw));
+            bq_push(2u, keep, v[h], w.qcap, sout, &ex.ctl->lc[nxt][C_SCOPE], g.V, ex.ctl, 25);
+        }
     }
     if constexpr (Ex::instr) {
         unsigned t = __reduce_add_sync(FULL, scanned);
@@ -616,8 +622,13 @@ struct SeedRanges {   // per-range pivots (selectPivots, scc_kernels.cu:4-19), w
 // frontier's vertices have more than bu_k * scope.n edges to expand.  lw < 0 selects the
 // load-balanced warp schedule for top-down steps, lw >= 0 the virtual-warp
 // schedule with W = 1 << lw.
+//
+// spare: a free vertex-sized buffer (or nullptr) that the first bottom-up
+// step fills with the vertices still unvisited in some direction; later
+// steps then take that shorter list as their scope (whole-GPU policy only).
 template <class Ex, class Seed>
-__device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed seed, bool bw, int lw, VList scope)
+__device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed seed, bool bw, int lw, VList scope,
+                       uint32_t *spare = nullptr)
 {
     const unsigned gsz = (lw < 0) ? 32u : (32u >> lw);
     const bool single = src.n == 1u && src.p == nullptr;
@@ -632,6 +643,7 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
             if (ex.leader()) {
                 atomicOr(&w.st[p], bits);
                 atomicAdd(&ex.ctl->n_pivot, 1ull);
+                w.smin[p] = p;   // p represents its SCC: the update passes fold the members in
             }
             // 64-entry pieces, one per warp, so the hub's lists spread over
             // the whole grid in one round of gathers
@@ -660,7 +672,10 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
             uint32_t v = act ? seed.vert(w, x) : x;
             bool lead = (lw <= 0) || ((lane_id() & ((1u << lw) - 1u)) == 0u);
             uint32_t r = 0;
-            if (act && lead) r = atomicOr(&w.st[v], bits) & RMASK;
+            if (act && lead) {
+                r = atomicOr(&w.st[v], bits) & RMASK;
+                w.smin[v] = v;   // v represents its SCC from here on
+            }
             if (lw > 0) r = __shfl_sync(FULL, r, lane_id() & ~((1u << lw) - 1u));
             unsigned m = __ballot_sync(FULL, act && lead);
             if (lane_id() == 0 && m) atomicAdd(&ex.ctl->n_pivot, (unsigned long long)__popc(m));
@@ -686,6 +701,7 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
         // walk the ids instead of the scope list when it holds most of them
         const VList psrc = 2ull * scope.n >= (unsigned long long)g.V ? VList{nullptr, g.V, 1u} : scope;
         const uint32_t nd = (puf || pub) ? (psrc.n + 63u) / 64u : 0u;
+        uint32_t *sout = (Ex::nbq > 2 && (puf || pub)) ? spare : nullptr;
         ok = run_pass(ex, (puf || pub) ? PH_BFS_PULL : PH_BFS, [&](unsigned, unsigned nxt) {
             const unsigned par = ex.gl & 1u, cp = par ^ 1u;
             // virtual-warp items take VWK groups of frontier vertices
@@ -695,7 +711,7 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
             const uint32_t items_b = pub ? 0u : (bw ? nhb + ngb : 0u);
             for (uint32_t it = ex.wid(); it < nd + items_f + items_b; it += ex.nwarps()) {
                 if (it < nd) {
-                    bfs_pull2(ex, g, w, puf, pub, psrc, it, par, nxt);
+                    bfs_pull2(ex, g, w, puf, pub, bw, psrc, it, par, nxt, sout);
                     continue;
                 }
                 const uint32_t it2 = it - nd;
@@ -739,10 +755,15 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
                     }
                 }
             }
-            bq_flush(2, w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_FQ], w.Q[1][par], &ex.ctl->lc[nxt][C_BQ], g.V,
-                     ex.ctl, &ex.ctl->lc[nxt][C_FE], &ex.ctl->lc[nxt][C_BE]);
+            bq_flush(sout ? 3u : 2u, w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_FQ], w.Q[1][par],
+                     &ex.ctl->lc[nxt][C_BQ], g.V, ex.ctl, &ex.ctl->lc[nxt][C_FE], &ex.ctl->lc[nxt][C_BE], sout,
+                     &ex.ctl->lc[nxt][C_SCOPE]);
         });
         if (!ok) return false;
+        if (sout) {   // the next bottom-up steps walk the shrunken scope
+            scope = VList{sout, last_count(ex, C_SCOPE), 0u};
+            spare = nullptr;
+        }
     }
 }
 
@@ -865,6 +886,7 @@ __device__ bool ph_hong_update(Ex &ex, const Graph &g, const Work &w, VList src,
                 }
                 if (single) mn = scc ? min(mn, v[j]) : mn;
                 else smin_fold(scc, p, v[j], w.smin);
+                bq_add_edges(0, surv ? __ldg(&g.Fr[v[j] + 1u]) - __ldg(&g.Fr[v[j]]) : 0u);
                 bq_push(0, surv, v[j], w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 15);
                 if (fold) {
                     // the new ranges are listed by their first bid (as in ph_pivots)
@@ -875,7 +897,7 @@ __device__ bool ph_hong_update(Ex &ex, const Graph &g, const Work &w, VList src,
             count_verts_n(ex, (unsigned)ok[0] + ok[1] + ok[2] + ok[3]);
         }
         if (single) block_min_atomic(mn, w.pivkey[0] ? &w.smin[key_vertex(w.pivkey[0])] : w.smin);
-        bq_flush(1, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], nullptr, nullptr, g.V, ex.ctl);
+        bq_flush(1, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], nullptr, nullptr, g.V, ex.ctl, &ex.ctl->lc[nxt][C_FE]);
     });
 }
 
@@ -899,15 +921,16 @@ __device__ bool ph_slota_first_update(Ex &ex, const Graph &g, const Work &w, VLi
                 bool surv = false, scc = false;
                 if (s[j] != DEAD) {
                     if ((s[j] & FVB) && (s[j] & BVB)) { w.st[v[j]] = DEAD; w.label[v[j]] = p; scc = true; }
-                    else { w.st[v[j]] = v[j]; surv = true; }
+                    else { w.st[v[j]] = v[j]; w.stamp[v[j]] = 0u; surv = true; }   // the colouring's work lists stamp them
                 }
                 mn = scc ? min(mn, v[j]) : mn;
+                bq_add_edges(0, surv ? __ldg(&g.Fr[v[j] + 1u]) - __ldg(&g.Fr[v[j]]) : 0u);
                 bq_push(0, surv, v[j], w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 16);
             }
             count_verts_n(ex, (unsigned)ok[0] + ok[1] + ok[2] + ok[3]);
         }
         block_min_atomic(mn, w.pivkey[0] ? &w.smin[p] : w.smin);   // mn stays 0xFFFFFFFF without a pivot
-        bq_flush(1, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], nullptr, nullptr, g.V, ex.ctl);
+        bq_flush(1, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], nullptr, nullptr, g.V, ex.ctl, &ex.ctl->lc[nxt][C_FE]);
     });
 }
 
@@ -933,11 +956,12 @@ __device__ bool ph_slota_peel_update(Ex &ex, const Graph &g, const Work &w, VLis
                     else { w.st[v[j]] = v[j]; surv = true; }
                 }
                 smin_fold(scc, c, v[j], w.smin);
+                bq_add_edges(0, surv ? __ldg(&g.Fr[v[j] + 1u]) - __ldg(&g.Fr[v[j]]) : 0u);
                 bq_push(0, surv, v[j], w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 17);
             }
             count_verts_n(ex, (unsigned)ok[0] + ok[1] + ok[2] + ok[3]);
         }
-        bq_flush(1, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], nullptr, nullptr, g.V, ex.ctl);
+        bq_flush(1, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], nullptr, nullptr, g.V, ex.ctl, &ex.ctl->lc[nxt][C_FE]);
     });
 }
 
@@ -981,7 +1005,9 @@ __device__ bool ph_pivots(Ex &ex, const Graph &g, const Work &w, VList src)
             uint32_t r = valid ? (w.st[v] & RMASK) : 0u;
             const bool first = range_max_atomic(valid, r, valid ? pivot_key(g, v) : 0ull, w.pivkey);
             warp_push(first, r, w.Q[0][par], &ex.ctl->lc[nxt][C_RNG], g.V + 1u, ex.ctl, 21);
+            bq_add_edges(0, valid ? __ldg(&g.Fr[v + 1u]) - __ldg(&g.Fr[v]) : 0u);
         }
+        bq_flush_edges(&ex.ctl->lc[nxt][C_FE]);   // out-arcs of the live list (the residual check)
     });
 }
 
@@ -993,9 +1019,249 @@ struct Carry {
     unsigned lsel;
     uint32_t nL;
     uint32_t nR;    // Hong: ranges listed by the last bidding pass (in Q[0][its parity])
+    uint32_t nE;    // out-arcs of the live vertices (tallied by the pass that listed them)
 };
 
-enum { RUN_DONE = 0, RUN_SWITCH = 1, RUN_ERROR = -1 };
+enum { RUN_DONE = 0, RUN_SWITCH = 1, RUN_RESIDUAL = 2, RUN_ERROR = -1 };
+
+// ---------------------------------------------------------------------
+// Small residuals: when the live vertices left for the main loop / the
+// colouring peels are few (at most RES_MAX_V, with at most RES_MAX_E
+// out-arcs), their SCCs are found on one CTA in shared memory instead of
+// by further whole-GPU passes.  SCCs never contain a vertex whose SCC is
+// already known, so the SCCs of the live vertices are those of the
+// subgraph they induce; every SCC found here counts as a pivot SCC, as the
+// reference counts each SCC its main loop / colouring finds once
+// (scc_WCC.cu:933-949, scc_Coloring.cu:640-652), so the counters and the
+// canonical labels are those of any complete run.
+//   pass 1 (all CTAs): live vertex L[i] gets the state word FV|BV|i (no
+//          other vertex has both bits at a loop head);
+//   pass 2 (all CTAs): the arcs between live vertices, as (i << 16) | j,
+//          into a work queue;
+//   then one CTA loads them into shared memory and peels SCCs by colour
+//   propagation (max of the local ids reachable on even peels, min on odd
+//   ones, so a chain is cut from either end) and a forward search inside
+//   each colour from its root, as scc_Coloring.cu:590-637 does, but with
+//   __syncthreads barriers between sweeps.
+// ---------------------------------------------------------------------
+constexpr uint32_t RES_MAX_V = 4096;
+constexpr uint32_t RES_MAX_E = 16384;
+
+__host__ __device__ __forceinline__ uint32_t res_al4(uint32_t x) { return (x + 3u) & ~3u; }
+// shared memory of the solver: gid, off, aux (u32), col (u16), flag (u8), adj (u16)
+__host__ __device__ __forceinline__ uint32_t res_smem_bytes(uint32_t n, uint32_t m)
+{
+    return 4u * n + 4u * (n + 1u) + 4u * n + res_al4(2u * n) + res_al4(n) + res_al4(2u * m);
+}
+
+// Uniform decision (same in every thread of the launch or CTA): solve the
+// live list on one CTA?  The solver uses the staging queues' shared memory.
+template <class Ex>
+__device__ __forceinline__ bool res_fits(const Graph &g, const Work &w, const Carry &cy)
+{
+    if (Ex::cluster || cy.nL == 0u || cy.nL > RES_MAX_V || cy.nE > RES_MAX_E || cy.nE > g.V + 1u) return false;
+    const uint32_t avail = Ex::nbq * (blockDim.x >> 5) * w.qcap * 4u;
+    return res_smem_bytes(cy.nL, cy.nE) <= avail;
+}
+
+// Block-wide exclusive prefix sum of a[0..len) in place (shared memory).
+// Every thread of the CTA calls it.
+__device__ __forceinline__ void block_excl_scan(uint32_t *a, uint32_t len)
+{
+    __shared__ uint32_t s_part[32];
+    const uint32_t per = (len + blockDim.x - 1u) / blockDim.x;
+    const uint32_t lo = threadIdx.x * per, hi = min(lo + per, len);
+    uint32_t sum = 0;
+    for (uint32_t i = lo; i < hi; i++) sum += a[i];
+    const uint32_t incl = warp_incl_scan(sum);
+    const unsigned wi = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (lane_id() == 31u) s_part[wi] = incl;
+    __syncthreads();
+    if (wi == 0) {
+        const uint32_t x = lane_id() < nw ? s_part[lane_id()] : 0u;
+        const uint32_t xs = warp_incl_scan(x);
+        if (lane_id() < nw) s_part[lane_id()] = xs - x;   // exclusive offset of each warp
+    }
+    __syncthreads();
+    uint32_t run = s_part[wi] + incl - sum;
+    for (uint32_t i = lo; i < hi; i++) {
+        const uint32_t x = a[i];
+        a[i] = run;
+        run += x;
+    }
+    __syncthreads();
+}
+
+// Passes 1 and 2 (every CTA of the policy).  On return the arcs are in
+// Q[1][(cy.gl - 1) & 1] and their number in the pass counter C_BQ.
+template <class Ex>
+__device__ bool res_extract(Ex &ex, const Graph &g, const Work &w, Carry &cy)
+{
+    const uint32_t *L = w.L[cy.lsel];
+    const uint32_t n = cy.nL;
+    if (!run_pass(ex, PH_RES_TAG, [&](unsigned, unsigned) {
+            for (uint32_t i = ex.tid(); i < n; i += ex.nthr()) w.st[L[i]] = FVB | BVB | i;
+        }))
+        return false;
+    const bool ok = run_pass(ex, PH_RES_EXTRACT, [&](unsigned, unsigned nxt) {
+        uint32_t *eb = w.Q[1][ex.gl & 1u];
+        for (uint32_t base = ex.wid() * 32u; base < n; base += ex.nwarps() * 32u) {
+            const uint32_t i = base + lane_id();
+            const bool valid = i < n;
+            const uint32_t v = valid ? L[i] : 0u;
+            const uint32_t beg = valid ? __ldg(&g.Fr[v]) : 0u, deg = valid ? __ldg(&g.Fr[v + 1u]) - beg : 0u;
+            auto fn = [&](bool ok2, uint32_t u, uint32_t src) {
+                bool hit = false;
+                uint32_t e = 0;
+                if (ok2) {
+                    const uint32_t s = w.st[guard_id(u, g.V, ex.ctl)];
+                    hit = (s & (FVB | BVB)) == (FVB | BVB);
+                    e = (src << 16) | (s & 0xFFFFu);
+                }
+                warp_push(hit, e, eb, &ex.ctl->lc[nxt][C_BQ], RES_MAX_E, ex.ctl, 24);
+            };
+            count_edges(ex, lbs_expand(beg, deg, i, g.Fc, fn));
+        }
+    });
+    cy.gl = ex.gl;
+    return ok;
+}
+
+// The solver (every thread of one CTA).  L[0..n): the live vertices;
+// eb[0..m): their arcs (i << 16) | j.  Writes every live vertex's
+// canonical label (LBL_SELF: the smallest id of its SCC) and DEAD state, and
+// adds the SCCs found to n_pivot.  Each peel removes at least the root with
+// the largest (or smallest) key, so at most n peels, each with at most n + 1
+// sweeps per fixpoint.
+static __device__ __noinline__ void res_solve(const Graph &g, const Work &w, const uint32_t *L, uint32_t n, const uint32_t *eb,
+                          uint32_t m, Ctl *ctl)
+{
+    constexpr uint8_t ALIVE = 1, VIS = 2;
+    char *sb = reinterpret_cast<char *>(&sccb_dsmem[BQ_HDR]);
+    uint32_t *gid = reinterpret_cast<uint32_t *>(sb);
+    uint32_t *off = gid + n;
+    uint32_t *aux = off + n + 1u;                  // fill cursor, then smallest member id per root
+    uint16_t *col = reinterpret_cast<uint16_t *>(aux + n);
+    uint8_t *flag = reinterpret_cast<uint8_t *>(sb + 12u * n + 4u + res_al4(2u * n));
+    uint16_t *adj = reinterpret_cast<uint16_t *>(sb + 12u * n + 4u + res_al4(2u * n) + res_al4(n));
+    __shared__ uint32_t s_alive, s_npiv, s_peels;
+    const uint32_t t = threadIdx.x, T = blockDim.x;
+    for (uint32_t i = t; i < n; i += T) {
+        gid[i] = L[i];
+        off[i] = 0u;
+        flag[i] = ALIVE;
+    }
+    if (t == 0) { off[n] = 0u; s_alive = n; s_npiv = 0u; s_peels = 0u; }
+    __syncthreads();
+    for (uint32_t k = t; k < m; k += T) atomicAdd(&off[eb[k] >> 16], 1u);
+    __syncthreads();
+    block_excl_scan(off, n + 1u);
+    for (uint32_t i = t; i < n; i += T) aux[i] = off[i];
+    __syncthreads();
+    for (uint32_t k = t; k < m; k += T) {
+        const uint32_t e = eb[k];
+        adj[atomicAdd(&aux[e >> 16], 1u)] = (uint16_t)(e & 0xFFFFu);
+    }
+    __syncthreads();
+    for (uint32_t i = t; i < n; i += T) aux[i] = 0xFFFFFFFFu;
+    __syncthreads();
+    bool failed = false;
+    for (uint32_t peel = 0;; peel++) {
+        if (s_alive == 0u) break;
+        if (peel > n + 1u) { failed = true; break; }
+        const bool up = (peel & 1u) == 0u;
+        for (uint32_t i = t; i < n; i += T)
+            if (flag[i] & ALIVE) col[i] = (uint16_t)(up ? i : n - 1u - i);
+        __syncthreads();
+        // colour = largest key reachable (scc_kernels.cu:539-564)
+        for (uint32_t sweep = 0;; sweep++) {
+            int ch = 0;
+            for (uint32_t i = t; i < n; i += T) {
+                if (!(flag[i] & ALIVE)) continue;
+                uint16_t c = col[i];
+                for (uint32_t e = off[i]; e < off[i + 1u]; e++) {
+                    const uint16_t j = adj[e];
+                    if ((flag[j] & ALIVE) && col[j] > c) c = col[j];
+                }
+                if (c > col[i]) { col[i] = c; ch = 1; }
+            }
+            if (!__syncthreads_or(ch)) break;
+            if (sweep > n + 1u) { failed = true; break; }
+        }
+        if (failed) break;
+        // roots keep their own key; the forward search inside each colour
+        // (scc_kernels.cu:567-610) marks their SCCs
+        for (uint32_t i = t; i < n; i += T)
+            if ((flag[i] & ALIVE) && col[i] == (up ? i : n - 1u - i)) flag[i] |= VIS;
+        __syncthreads();
+        for (uint32_t sweep = 0;; sweep++) {
+            int ch = 0;
+            for (uint32_t i = t; i < n; i += T) {
+                if ((flag[i] & (ALIVE | VIS)) != (ALIVE | VIS)) continue;
+                for (uint32_t e = off[i]; e < off[i + 1u]; e++) {
+                    const uint16_t j = adj[e];
+                    if ((flag[j] & (ALIVE | VIS)) == ALIVE && col[j] == col[i]) { flag[j] |= VIS; ch = 1; }
+                }
+            }
+            if (!__syncthreads_or(ch)) break;
+            if (sweep > n + 1u) { failed = true; break; }
+        }
+        if (failed) break;
+        uint32_t done = 0, roots = 0;
+        for (uint32_t i = t; i < n; i += T) {
+            if ((flag[i] & (ALIVE | VIS)) != (ALIVE | VIS)) continue;
+            const uint32_t r = up ? col[i] : n - 1u - col[i];
+            atomicMin(&aux[r], gid[i]);
+            col[i] = (uint16_t)r;   // the root, from here on
+            flag[i] = 0;
+            done++;
+            roots += (r == i) ? 1u : 0u;
+        }
+        done = __reduce_add_sync(FULL, done);
+        roots = __reduce_add_sync(FULL, roots);
+        if (lane_id() == 0 && done) { atomicSub(&s_alive, done); atomicAdd(&s_npiv, roots); }
+        if (t == 0) s_peels = peel + 1u;
+        __syncthreads();
+    }
+    if (failed) {
+        if (t == 0) set_error(ctl, E_NOT_CONVERGED, 71);
+        return;
+    }
+    for (uint32_t i = t; i < n; i += T) {
+        w.label[gid[i]] = LBL_SELF | aux[col[i]];
+        w.st[gid[i]] = DEAD;
+    }
+    if (t == 0) {
+        atomicAdd(&ctl->n_pivot, (unsigned long long)s_npiv);
+        atomicAdd(&ctl->outer, s_peels);
+    }
+    __syncthreads();
+}
+
+// Records the solver as one more pass in the pass trace (one CTA).
+__device__ __forceinline__ void res_trace(Ctl *ctl, unsigned gl, uint32_t n)
+{
+    if (threadIdx.x == 0 && ctl->trace && gl < ctl->trace_cap) {
+        ctl->trace[2 * gl] = gtimer();
+        ctl->trace[2 * gl + 1] = (unsigned long long)PH_RES_SOLVE | ((unsigned long long)n << 8);
+    }
+}
+
+// Residual path at a main-loop / peel head.  On the whole-GPU policy it
+// returns RUN_RESIDUAL after the two passes (CTA 0 then solves and the
+// others leave); on one CTA it also solves and returns RUN_DONE.
+template <class Ex>
+__device__ int residual(Ex &ex, const Graph &g, const Work &w, Carry &cy)
+{
+    if (!res_extract(ex, g, w, cy)) return RUN_ERROR;
+    if (Ex::grid) return RUN_RESIDUAL;
+    res_solve(g, w, w.L[cy.lsel], cy.nL, w.Q[1][(cy.gl - 1u) & 1u], last_count(ex, C_BQ), ex.ctl);
+    res_trace(ex.ctl, ex.gl, cy.nL);
+    ex.gl++;
+    cy.gl = ex.gl;
+    cy.nL = 0u;
+    return ex.sync() ? RUN_DONE : RUN_ERROR;
+}
 
 // Hong main loop (scc_WCC.cu:851-930): per-range pivots, FW-BW, update,
 // until no vertex is left.  Entry: live list L[lsel] with nL entries and
@@ -1004,14 +1270,16 @@ template <class Ex>
 __device__ int hong_loop(Ex &ex, const Graph &g, const Work &w, Carry &cy, uint32_t tail_n)
 {
     while (cy.nL > 0u) {
+        if (res_fits<Ex>(g, w, cy)) return residual(ex, g, w, cy);
         if (Ex::grid && cy.nL <= tail_n) { cy.gl = ex.gl; return RUN_SWITCH; }
         if (ex.leader()) ex.ctl->outer++;
         const VList L{w.L[cy.lsel], cy.nL, 0u};
         const VList R{w.Q[0][(ex.gl & 1u) ^ 1u], cy.nR, 0u};   // written by the previous pass
-        if (!ph_bfs(ex, g, w, R, SeedRanges{}, true, -1, L)) return RUN_ERROR;
+        if (!ph_bfs(ex, g, w, R, SeedRanges{}, true, -1, L, w.L[cy.lsel ^ 1u])) return RUN_ERROR;
         if (!ph_hong_update(ex, g, w, L, w.L[cy.lsel ^ 1u], false, true)) return RUN_ERROR;
         cy.nL = last_count(ex, C_LIST);
         cy.nR = last_count(ex, C_RNG);
+        cy.nE = last_count(ex, C_FE);
         cy.lsel ^= 1u;
         cy.gl = ex.gl;
     }
@@ -1065,7 +1333,8 @@ __device__ bool first_fwbw(Ex &ex, const Graph &g, const Work &w, int lw, VList 
 {
     const unsigned long long k = vld64(&w.pivkey[0]);
     const uint32_t p = k ? key_vertex(k) : 0u;
-    return ph_bfs(ex, g, w, VList{nullptr, k ? 1u : 0u, p}, SeedOne{p}, true, lw, scope);
+    // L[1] is written only by the update pass after this search
+    return ph_bfs(ex, g, w, VList{nullptr, k ? 1u : 0u, p}, SeedOne{p}, true, lw, scope, w.L[1]);
 }
 
 // vHong / wHong up to the main loop (scc_WCC.cu:573-848): trim1*, first
@@ -1094,6 +1363,7 @@ __device__ int hong_front(Ex &ex, const Graph &g, const Work &w, bool t1, bool t
     if (!ph_propagate<false>(ex, g, w, L)) return RUN_ERROR;
     if (!ph_pivots(ex, g, w, L)) return RUN_ERROR;
     cy.nR = last_count(ex, C_RNG);
+    cy.nE = last_count(ex, C_FE);
     cy.gl = ex.gl;
     return RUN_DONE;
 }
@@ -1115,6 +1385,7 @@ __device__ int slota_front(Ex &ex, const Graph &g, const Work &w, bool t1, int l
     if (!ph_slota_first_update(ex, g, w, scope, w.L[1])) return RUN_ERROR;
     cy.lsel = 1u;
     cy.nL = last_count(ex, C_LIST);
+    cy.nE = last_count(ex, C_FE);
     cy.gl = ex.gl;
     return RUN_DONE;
 }
@@ -1125,13 +1396,15 @@ template <class Ex>
 __device__ int slota_peels(Ex &ex, const Graph &g, const Work &w, Carry &cy, uint32_t tail_n)
 {
     while (cy.nL > 0u) {
+        if (res_fits<Ex>(g, w, cy)) return residual(ex, g, w, cy);
         if (Ex::grid && cy.nL <= tail_n) { cy.gl = ex.gl; return RUN_SWITCH; }
         if (ex.leader()) ex.ctl->outer++;
         const VList L{w.L[cy.lsel], cy.nL, 0u};
         if (!ph_propagate<true>(ex, g, w, L)) return RUN_ERROR;
-        if (!ph_bfs(ex, g, w, L, SeedRoot{}, false, -1, L)) return RUN_ERROR;
+        if (!ph_bfs(ex, g, w, L, SeedRoot{}, false, -1, L, w.L[cy.lsel ^ 1u])) return RUN_ERROR;
         if (!ph_slota_peel_update(ex, g, w, L, w.L[cy.lsel ^ 1u])) return RUN_ERROR;
         cy.nL = last_count(ex, C_LIST);
+        cy.nE = last_count(ex, C_FE);
         cy.lsel ^= 1u;
         cy.gl = ex.gl;
     }

@@ -133,11 +133,21 @@ int scc_derive_reverse(scc_context *ctx, const uint32_t *Fr, const uint32_t *Fc,
  *                         bu_k * (vertices the search can reach) (default 2,
  *                         0 = never)
  *   "qcap"                entries of each warp's shared-memory staging slice
- *                         (32..768; 2 queues x 32 warps x qcap x 4 bytes)
+ *                         (32..576; 3 queues x 32 warps x qcap x 4 bytes on
+ *                         the whole-GPU kernel, 2 queues on one CTA)
  *   "cluster_check"       batched launches with clusters use a software
  *                         barrier in global memory whose waits end after
  *                         timeout_ms with SCC_ERR_TIMEOUT (a check mode;
- *                         default 0: the hardware cluster barrier) */
+ *                         default 0: the hardware cluster barrier)
+ *   "max_passes"          a run stops with SCC_ERR_NOT_CONVERGED once it has
+ *                         made this many device passes (0, the default: no
+ *                         cap beyond the V + 2 passes of every loop)
+ *   "test_withhold_arrival"  failure-detection test hook: with k + 1, one CTA
+ *                         of a whole-GPU launch (or of a cluster in check
+ *                         mode) withholds its barrier arrival at pass k, so
+ *                         every wait of that barrier runs out after
+ *                         timeout_ms and the run ends with SCC_ERR_TIMEOUT;
+ *                         0 (the default) turns it off */
 int scc_set_tuning(scc_context *ctx, const char *key, long long value);
 
 /* Per-pass trace of the last run (enable with scc_set_tuning(ctx, "trace",
@@ -237,7 +247,8 @@ int scc_server_destroy(scc_server *s);
 typedef struct {
     uint32_t V, E;
     uint32_t *Fr, *Fc, *Br, *Bc;
-    uint32_t *Pr;           /* METIS partition ids, zero-filled (detectSCC only) */
+    uint32_t *Pr;           /* METIS partition ids (detectSCC only): read from the file named by the
+                               environment variable SCC_METIS_PARTITION when it is set, else zero-filled */
 } scc_host_graph;
 
 /* Read a GTgraph text file (load.cpp:12-140 semantics) or a binary CSR file
@@ -249,6 +260,19 @@ int scc_save_binary(const char *path, const scc_host_graph *g);
 int scc_graph_from_arcs(uint32_t V, uint64_t E, const uint32_t *src, const uint32_t *dst,
                         scc_host_graph *out);
 void scc_free_host_graph(scc_host_graph *g);
+
+/* ---- METIS input converter and partitions ------------------------------ */
+/* Replaces the reference's converter tool (MetisInput.cpp:12-141, its
+ * loadFullGraph + writer): writes g in that tool's layout -- a line "V E",
+ * then for every vertex 1..V one line with its out-neighbours (forward list
+ * order) followed by its in-neighbours (reverse list order), each number
+ * followed by one space (MetisInput.cpp:114-131).  Duplicate arcs appear as
+ * often as they occur, as there. */
+int scc_save_metis(const char *path, const scc_host_graph *g);
+/* Reads a METIS partition file (one partition id per vertex, whitespace
+ * separated, load.cpp:115-130) into Pr[1..V]; Pr[0] and Pr[V+1] are set to
+ * 0.  Pr must hold V+2 entries. */
+int scc_load_partition(const char *path, uint32_t V, uint32_t *Pr);
 
 /* ---- reference-compatible driver call ----------------------------------- */
 /* Runs one of the reference drivers with its exact stdout: for 'g' the line
