@@ -64,6 +64,8 @@ struct __align__(128) Ctl {
     unsigned long long *trace;                     // optional: 2 words per pass
     unsigned trace_cap;
     unsigned labels_done;                          // the SCC kernel wrote the canonical labels itself
+    unsigned first_min;                            // smallest member of the first pivot's SCC when its members
+                                                   // keep the FV|BV mark (lazy Slota update); ~0 before
 };
 
 // Phase ids recorded in the pass trace.
@@ -101,6 +103,7 @@ struct Work {
     uint32_t *smin;             // smin[r] = smallest member id of the SCC represented by r; set to r
                                 // when r becomes a representative (its seed pass), then folded
     uint32_t *L[2];
+    uint32_t *S[2];             // whole-GPU path: lists of the shrinking bottom-up scope (nullptr elsewhere)
     uint32_t *Q[2][2];          // [direction][parity]
     uint2 *H[2][2];             // heavy chunks (vertex, chunk) [direction][parity]
     uint32_t hcap;
@@ -129,6 +132,7 @@ __host__ __device__ inline size_t carve_work(char *base, uint32_t V, uint32_t E,
         w->smin = (uint32_t *)(base + 3 * va);
         w->L[0] = (uint32_t *)(base + 4 * va);
         w->L[1] = (uint32_t *)(base + 5 * va);
+        w->S[0] = w->S[1] = nullptr;
         w->Q[0][0] = (uint32_t *)(base + 6 * va);
         w->Q[0][1] = (uint32_t *)(base + 7 * va);
         w->Q[1][0] = (uint32_t *)(base + 8 * va);
@@ -455,9 +459,11 @@ __device__ __forceinline__ void warp_push(bool pred, uint32_t val, uint32_t *q, 
 // warp with one global atomicAdd per qcap entries, and bq_flush writes the
 // rest of all slices with one global atomicAdd per CTA and pass.  This keeps
 // the global queue tail from becoming a same-address atomic hot spot.
+__device__ __forceinline__ uint32_t *cta_first_min();
 __device__ __forceinline__ void bq_init()
 {
     for (unsigned i = threadIdx.x; i < BQ_HDR; i += blockDim.x) sccb_dsmem[i] = 0u;
+    if (threadIdx.x == 0) *cta_first_min() = 0xFFFFFFFFu;
     __syncthreads();
 }
 
@@ -530,6 +536,30 @@ __device__ __forceinline__ void bq_flush(unsigned nq, uint32_t qcap, uint32_t *g
         __syncwarp();
         if (lane_id() == 0) sccb_dsmem[BQ_CNT + qi * BQ_WARPS + wi] = 0u;
     }
+}
+
+// Per-CTA minimum of the vertices whose second visited bit (FV then BV or
+// BV then FV) was set by this CTA: the members of the first pivot's SCC
+// during the first search.  Cleared at kernel entry (bq_init).
+__device__ __forceinline__ uint32_t *cta_first_min()
+{
+    __shared__ uint32_t s_first_min;
+    return &s_first_min;
+}
+// old: the state word before an atomicOr of `bits`: v if that atomicOr
+// completed both visited bits, else ~0.
+__device__ __forceinline__ uint32_t completed(uint32_t old, uint32_t bits, uint32_t v)
+{
+    return ((old & (FVB | BVB)) != (FVB | BVB) && ((old | bits) & (FVB | BVB)) == (FVB | BVB)) ? v : 0xFFFFFFFFu;
+}
+// Folds the warp's smallest completed vertex into the CTA's minimum: one
+// warp reduction, and a shared-memory atomic only when it lowers the CTA's
+// current value (the first SCC's smallest member is found early, so almost
+// every call ends at the comparison).  All 32 lanes call.
+__device__ __forceinline__ void fold_completed(uint32_t cand)
+{
+    const uint32_t m = __reduce_min_sync(0xFFFFFFFFu, cand);
+    if ((threadIdx.x & 31u) == 0u && m < *(volatile uint32_t *)cta_first_min()) atomicMin(cta_first_min(), m);
 }
 
 // Adds the CTA's frontier-edge tally of queue 0 (word 12) to *ecnt and

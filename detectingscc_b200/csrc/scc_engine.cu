@@ -44,8 +44,11 @@ struct Params {
 // non-coherent read-only path.
 constexpr uint32_t LABEL_UNROLL = 4;
 
-__device__ __forceinline__ void canon_labels(const uint32_t *label, const uint32_t *smin, uint32_t *out, uint32_t V,
-                                             uint32_t tid, uint32_t n)
+// A vertex whose state still carries both visited bits with range 0 is a
+// member of the first pivot's SCC left marked by the lazy Slota update; its
+// label is first_min.
+__device__ __forceinline__ void canon_labels(const uint32_t *label, const uint32_t *smin, const uint32_t *st,
+                                             uint32_t first_min, uint32_t *out, uint32_t V, uint32_t tid, uint32_t n)
 {
     for (uint32_t v0 = tid + 1u; v0 <= V; v0 += LABEL_UNROLL * n) {
         uint32_t l[LABEL_UNROLL];
@@ -53,6 +56,7 @@ __device__ __forceinline__ void canon_labels(const uint32_t *label, const uint32
         for (uint32_t j = 0; j < LABEL_UNROLL; ++j) {
             const uint32_t v = v0 + j * n;
             l[j] = v <= V ? label[v] : 0xFFFFFFFFu;
+            if (v <= V && st[v] == (FVB | BVB)) l[j] = LBL_SELF | first_min;
         }
 #pragma unroll
         for (uint32_t j = 0; j < LABEL_UNROLL; ++j)
@@ -67,7 +71,7 @@ __device__ __forceinline__ void canon_labels(const uint32_t *label, const uint32
 
 __device__ __forceinline__ void write_labels(const Work &w, uint32_t V, uint32_t *out, uint32_t tid, uint32_t n)
 {
-    canon_labels(w.label, w.smin, out, V, tid, n);
+    canon_labels(w.label, w.smin, w.st, *(volatile const uint32_t *)&w.ctl->first_min, out, V, tid, n);
 }
 
 // ---------------------------------------------------------------------
@@ -141,10 +145,11 @@ __global__ void __launch_bounds__(BLOCK_THREADS, 1) k_scc_block(Params p)
 // which the update passes fold into smin[representative].
 // Skipped when the SCC kernel already wrote them (ctl->labels_done).
 __global__ void k_canon_write(const uint32_t *__restrict__ label, const uint32_t *__restrict__ smin,
-                              uint32_t *__restrict__ out, uint32_t V, const Ctl *ctl)
+                              const uint32_t *__restrict__ st, uint32_t *__restrict__ out, uint32_t V, const Ctl *ctl)
 {
     if (ctl && ctl->labels_done) return;
-    canon_labels(label, smin, out, V, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+    canon_labels(label, smin, st, ctl ? ctl->first_min : 0xFFFFFFFFu, out, V, blockIdx.x * blockDim.x + threadIdx.x,
+                 gridDim.x * blockDim.x);
 }
 
 // CTAs of 256 threads for k_canon_write: one round of LABEL_UNROLL vertices
@@ -199,7 +204,7 @@ namespace {
 
 // Offsets of the whole-graph workspace (all 256-byte aligned).
 struct WsLayout {
-    size_t st, label, stamp, smin, L0, L1, Q[4], H[4], piv, ctl, need, hcap;
+    size_t st, label, stamp, smin, L0, L1, S0, S1, Q[4], H[4], piv, ctl, need, hcap;
 };
 
 WsLayout ws_layout(uint32_t V, uint32_t E)
@@ -211,6 +216,7 @@ WsLayout ws_layout(uint32_t V, uint32_t E)
     auto take = [&](size_t bytes) { size_t off = need; need = align_up(need + bytes, 256); return off; };
     o.st = take(n1 * 4); o.label = take(n1 * 4); o.stamp = take(n1 * 4); o.smin = take(n1 * 4);
     o.L0 = take(n1 * 4); o.L1 = take(n1 * 4);
+    o.S0 = take(n1 * 4); o.S1 = take(n1 * 4);
     for (int i = 0; i < 4; i++) o.Q[i] = take(n1 * 4);
     for (int i = 0; i < 4; i++) o.H[i] = take(o.hcap * sizeof(uint2));
     o.piv = take((4 * n1 + 8) * 8);
@@ -246,6 +252,8 @@ int scc_ctx_reserve(scc_context *ctx, uint32_t V, uint32_t E)
     w.smin = (uint32_t *)(b + o_smin);
     w.L[0] = (uint32_t *)(b + o_L0);
     w.L[1] = (uint32_t *)(b + o_L1);
+    w.S[0] = (uint32_t *)(b + o.S0);
+    w.S[1] = (uint32_t *)(b + o.S1);
     w.Q[0][0] = (uint32_t *)(b + o_Q[0]);
     w.Q[0][1] = (uint32_t *)(b + o_Q[1]);
     w.Q[1][0] = (uint32_t *)(b + o_Q[2]);
@@ -458,6 +466,7 @@ extern "C" int scc_run(scc_context *ctx, const scc_csr_view *gv, int algo, uint3
 
     // control block: zeroed, then the timeout
     memset(ctx->hctl, 0, sizeof(Ctl));
+    ctx->hctl->first_min = 0xFFFFFFFFu;
     ctx->hctl->timeout_ns = (unsigned long long)ctx->timeout_ms * 1000000ull;
     ctx->hctl->trace = ctx->dtrace;
     ctx->hctl->trace_cap = ctx->dtrace ? ctx->trace_cap : 0u;
@@ -497,7 +506,8 @@ extern "C" int scc_run(scc_context *ctx, const scc_csr_view *gv, int algo, uint3
     launches++;
     CK(cudaEventRecord(ctx->ev[2], st));
     if (dout) {
-        k_canon_write<<<canon_ctas(V), 256, 0, st>>>(ctx->work.label, ctx->work.smin, dout, V, ctx->work.ctl);
+        k_canon_write<<<canon_ctas(V), 256, 0, st>>>(ctx->work.label, ctx->work.smin, ctx->work.st, dout, V,
+                                                     ctx->work.ctl);
         launches += 1;
         CK(cudaGetLastError());
         if (!dev) CK(cudaMemcpyAsync(labels_out, dout, (size_t)V * 4, cudaMemcpyDeviceToHost, st));
@@ -590,7 +600,7 @@ int sccb_launch_block_path(const Graph &g, const Work &w, int t1, int t2, int lw
     void *args[] = {&p};
     cudaError_t e = cudaLaunchKernel(fn, dim3(1), dim3(BLOCK_THREADS), args, smem, st);
     if (e != cudaSuccess) return cuda_status(e);
-    k_canon_write<<<canon_ctas(g.V), 256, 0, st>>>(w.label, w.smin, dout, g.V, nullptr);
+    k_canon_write<<<canon_ctas(g.V), 256, 0, st>>>(w.label, w.smin, w.st, dout, g.V, w.ctl);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_status(e);
     *launches = 2;

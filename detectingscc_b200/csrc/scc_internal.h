@@ -38,7 +38,8 @@ struct scc_context {
     uint32_t block_max_edges = 262144;
     uint32_t timeout_ms = 4000;          // bound on any single grid-barrier wait
     int max_blocks_per_sm = 0;           // 0 = occupancy limit
-    uint32_t qcap = 512;                 // per-warp staging slice entries (up to 3 queues x 32 warps in shared memory)
+    uint32_t qcap = 320;                 // per-warp staging slice entries (up to 3 queues x 32 warps in shared memory;
+                                         // larger slices shrink the L1 data cache and slow the gathers)
     uint32_t bu_k = 2;                   // bottom-up BFS step when frontier edges > bu_k * scope (0 = off)
     int cluster_check = 0;               // batched launches: bounded software cluster barriers (check mode)
     uint32_t max_passes = 0;             // a run stops with SCC_ERR_NOT_CONVERGED after this many passes (0: no cap)

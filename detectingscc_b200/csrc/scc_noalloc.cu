@@ -130,6 +130,7 @@ __global__ void k_noalloc_ctl_init(Ctl *c, unsigned long long timeout_ns)
 {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         memset(c, 0, sizeof(Ctl));
+        c->first_min = 0xFFFFFFFFu;
         c->timeout_ns = timeout_ns;
     }
 }
@@ -183,6 +184,7 @@ extern "C" int scc_run_noalloc(const scc_csr_view *gv, int algo, uint32_t flags,
     w.smin = (uint32_t *)take(n1 * 4);
     w.L[0] = (uint32_t *)take(n1 * 4);
     w.L[1] = (uint32_t *)take(n1 * 4);
+    w.S[0] = w.S[1] = nullptr;   // the single-CTA kernel keeps no shrinking scope
     w.Q[0][0] = (uint32_t *)take(n1 * 4);
     w.Q[0][1] = (uint32_t *)take(n1 * 4);
     w.Q[1][0] = (uint32_t *)take(n1 * 4);

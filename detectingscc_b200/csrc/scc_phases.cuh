@@ -365,11 +365,17 @@ __device__ __forceinline__ void bfs_edge_visit(Ex &ex, const Graph &g, const Wor
 {
     const uint32_t bit = dir ? BVB : FVB;
     bool claim = false;
+    uint32_t done = 0xFFFFFFFFu;
     if (valid) {
         nbr = guard_id(nbr, g.V, ex.ctl);
         uint32_t s = w.st[nbr];
-        if ((s & (RMASK | bit)) == r) claim = !(atomicOr(&w.st[nbr], bit) & bit);
+        if ((s & (RMASK | bit)) == r) {
+            const uint32_t o = atomicOr(&w.st[nbr], bit);
+            claim = !(o & bit);
+            done = completed(o, bit, nbr);
+        }
     }
+    fold_completed(done);
     const uint32_t *Rn = dir ? g.Br : g.Fr;
     bq_add_edges((unsigned)dir, claim ? __ldg(&Rn[nbr + 1]) - __ldg(&Rn[nbr]) : 0u);
     bq_push((unsigned)dir, claim, nbr, w.qcap, w.Q[dir][par], &ex.ctl->lc[nxt][C_FQ + dir], g.V, ex.ctl, 13);
@@ -392,6 +398,7 @@ __device__ __forceinline__ void bfs_edge_visit2(Ex &ex, const Graph &g, const Wo
     const uint32_t o0 = t0 ? atomicOr(&w.st[n0], bit) : bit;
     const uint32_t o1 = t1 ? atomicOr(&w.st[n1], bit) : bit;
     const bool c0 = !(o0 & bit), c1 = !(o1 & bit);
+    fold_completed(min(c0 ? completed(o0, bit, n0) : 0xFFFFFFFFu, c1 ? completed(o1, bit, n1) : 0xFFFFFFFFu));
     // edges the claimed vertices will expand next (direction-switch rule)
     const uint32_t *Rn = dir ? g.Br : g.Fr;
     unsigned e = 0;
@@ -488,10 +495,10 @@ __device__ __forceinline__ void chunk_expand(Ex &ex, const uint32_t *__restrict_
 // find a visited neighbour of its own range if its range is being
 // searched, so walking ids reaches the same set as walking the scope.
 //
-// With sout set (whole-GPU policy, first bottom-up step of a search), every
-// live vertex of the item that is still unvisited in a direction of the
-// search is appended to sout (staging queue 2): the scope of the next
-// bottom-up step, which then walks only those instead of the whole scope.
+// With sout set (whole-GPU policy), every live vertex of the item that is
+// still unvisited in a direction of the search is appended to sout (staging
+// queue 2): the scope of the next bottom-up step, which then walks only
+// those instead of the whole scope.
 template <class Ex>
 __device__ __forceinline__ void bfs_pull2(Ex &ex, const Graph &g, const Work &w, bool puf, bool pub, bool bw,
                                           VList src, uint32_t k, unsigned par, unsigned nxt, uint32_t *sout)
@@ -578,7 +585,7 @@ __device__ __forceinline__ void bfs_pull2(Ex &ex, const Graph &g, const Work &w,
 #pragma unroll
     for (int h = 0; h < 2; h++) {
         const uint32_t bits = (found[2 * h] ? FVB : 0u) | (found[2 * h + 1] ? BVB : 0u);
-        if (bits) atomicOr(&w.st[v[h]], bits);
+        fold_completed(bits ? completed(atomicOr(&w.st[v[h]], bits), bits, v[h]) : 0xFFFFFFFFu);
         // frontier edges of the next level: out-degree forward, in-degree backward
         if (puf) bq_add_edges(0u, found[2 * h] ? __ldg(&g.Fr[v[h] + 1u]) - __ldg(&g.Fr[v[h]]) : 0u);
         if (pub) bq_add_edges(1u, found[2 * h + 1] ? __ldg(&g.Br[v[h] + 1u]) - __ldg(&g.Br[v[h]]) : 0u);
@@ -623,13 +630,17 @@ struct SeedRanges {   // per-range pivots (selectPivots, scc_kernels.cu:4-19), w
 // load-balanced warp schedule for top-down steps, lw >= 0 the virtual-warp
 // schedule with W = 1 << lw.
 //
-// spare: a free vertex-sized buffer (or nullptr) that the first bottom-up
-// step fills with the vertices still unvisited in some direction; later
-// steps then take that shorter list as their scope (whole-GPU policy only).
+// On the whole-GPU policy every bottom-up step also lists the vertices of
+// its scope still unvisited in some direction (into w.S[0], w.S[1] in
+// turn): the next bottom-up step walks that shorter list, and the Beamer
+// rule weighs the frontier against it.  *last (optional) receives the scope
+// at the end: every live vertex of the original scope that is not visited
+// in both directions is in it.
 template <class Ex, class Seed>
 __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed seed, bool bw, int lw, VList scope,
-                       uint32_t *spare = nullptr)
+                       VList *last = nullptr)
 {
+    unsigned nshrink = 0;
     const unsigned gsz = (lw < 0) ? 32u : (32u >> lw);
     const bool single = src.n == 1u && src.p == nullptr;
     bool ok = run_pass(ex, PH_BFS0, [&](unsigned, unsigned nxt) {
@@ -641,7 +652,7 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
             // takes CH-entry chunks of its out- and in-list in this pass
             const uint32_t p = src.base;
             if (ex.leader()) {
-                atomicOr(&w.st[p], bits);
+                if (completed(atomicOr(&w.st[p], bits), bits, p) == p) atomicMin(cta_first_min(), p);
                 atomicAdd(&ex.ctl->n_pivot, 1ull);
                 w.smin[p] = p;   // p represents its SCC: the update passes fold the members in
             }
@@ -672,10 +683,14 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
             uint32_t v = act ? seed.vert(w, x) : x;
             bool lead = (lw <= 0) || ((lane_id() & ((1u << lw) - 1u)) == 0u);
             uint32_t r = 0;
+            uint32_t done = 0xFFFFFFFFu;
             if (act && lead) {
-                r = atomicOr(&w.st[v], bits) & RMASK;
+                const uint32_t o = atomicOr(&w.st[v], bits);
+                done = completed(o, bits, v);
+                r = o & RMASK;
                 w.smin[v] = v;   // v represents its SCC from here on
             }
+            fold_completed(done);
             if (lw > 0) r = __shfl_sync(FULL, r, lane_id() & ~((1u << lw) - 1u));
             unsigned m = __ballot_sync(FULL, act && lead);
             if (lane_id() == 0 && m) atomicAdd(&ex.ctl->n_pivot, (unsigned long long)__popc(m));
@@ -690,7 +705,10 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
     for (unsigned lev = 1;; lev++) {
         const uint32_t nf = last_count(ex, C_FQ), nb = last_count(ex, C_BQ);
         const uint32_t nhf = last_count(ex, C_FH), nhb = last_count(ex, C_BH);
-        if (nf + nb + nhf + nhb == 0u) return true;
+        if (nf + nb + nhf + nhb == 0u) {
+            if (last) *last = scope;
+            return true;
+        }
         if (lev > g.V + 2u) { if (ex.leader()) set_error(ex.ctl, E_NOT_CONVERGED, 40); return false; }
         // Beamer's rule: bottom-up when the frontier has more edges to
         // expand than the scope has vertices to test (times bu_k)
@@ -701,7 +719,9 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
         // walk the ids instead of the scope list when it holds most of them
         const VList psrc = 2ull * scope.n >= (unsigned long long)g.V ? VList{nullptr, g.V, 1u} : scope;
         const uint32_t nd = (puf || pub) ? (psrc.n + 63u) / 64u : 0u;
-        uint32_t *sout = (Ex::nbq > 2 && (puf || pub)) ? spare : nullptr;
+        // one shrink per search: a second bottom-up step over the shrunken
+        // scope costs more than the top-down steps it would replace
+        uint32_t *sout = (Ex::nbq > 2 && (puf || pub) && nshrink == 0u) ? w.S[0] : nullptr;
         ok = run_pass(ex, (puf || pub) ? PH_BFS_PULL : PH_BFS, [&](unsigned, unsigned nxt) {
             const unsigned par = ex.gl & 1u, cp = par ^ 1u;
             // virtual-warp items take VWK groups of frontier vertices
@@ -762,7 +782,7 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
         if (!ok) return false;
         if (sout) {   // the next bottom-up steps walk the shrunken scope
             scope = VList{sout, last_count(ex, C_SCOPE), 0u};
-            spare = nullptr;
+            nshrink++;
         }
     }
 }
@@ -934,6 +954,37 @@ __device__ bool ph_slota_first_update(Ex &ex, const Graph &g, const Work &w, VLi
     });
 }
 
+// The same update on the whole-GPU policy, where the search kept a
+// shrinking scope: members of the first SCC (both visited bits) keep that
+// mark as their state -- no later phase treats it as live, and the label
+// write maps it to the SCC's smallest member, Ctl::first_min, which every
+// CTA folds in here from the completions it saw -- so only the search's
+// final scope is walked, not every vertex the search could reach.
+template <class Ex>
+__device__ bool ph_slota_first_update_lazy(Ex &ex, const Graph &g, const Work &w, VList src, uint32_t *Lout)
+{
+    return run_pass(ex, PH_SLOTA_FIRST_UPDATE, [&](unsigned, unsigned nxt) {
+        for (uint32_t base = ex.wid() * 128u; base < src.n; base += ex.nwarps() * 128u) {
+            uint32_t v[4], s[4];
+            bool ok[4];
+            load_list4(src, base + 4u * lane_id(), v, ok);
+#pragma unroll
+            for (int j = 0; j < 4; j++) s[j] = ok[j] ? w.st[v[j]] : DEAD;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const bool surv = s[j] != DEAD && (s[j] & (FVB | BVB)) != (FVB | BVB);
+                if (surv) { w.st[v[j]] = v[j]; w.stamp[v[j]] = 0u; }
+                bq_add_edges(0, surv ? __ldg(&g.Fr[v[j] + 1u]) - __ldg(&g.Fr[v[j]]) : 0u);
+                bq_push(0, surv, v[j], w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 16);
+            }
+            count_verts_n(ex, (unsigned)ok[0] + ok[1] + ok[2] + ok[3]);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0 && *cta_first_min() != 0xFFFFFFFFu) atomicMin(&ex.ctl->first_min, *cta_first_min());
+        bq_flush(1, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], nullptr, nullptr, g.V, ex.ctl, &ex.ctl->lc[nxt][C_FE]);
+    });
+}
+
 // Slota peel end (updateColoring, scc_kernels.cu:614-623; fwdColoring's
 // rangeSet, :607): visited vertices belong to their root's SCC; the rest
 // restart from their own colour and form the next live list.
@@ -1034,8 +1085,9 @@ enum { RUN_DONE = 0, RUN_SWITCH = 1, RUN_RESIDUAL = 2, RUN_ERROR = -1 };
 // reference counts each SCC its main loop / colouring finds once
 // (scc_WCC.cu:933-949, scc_Coloring.cu:640-652), so the counters and the
 // canonical labels are those of any complete run.
-//   pass 1 (all CTAs): live vertex L[i] gets the state word FV|BV|i (no
-//          other vertex has both bits at a loop head);
+//   pass 1 (all CTAs): live vertex L[i] gets the state word FV|BV|(i + 1)
+//          (at a loop head the only other vertices with both bits are the
+//          first SCC's members, marked FV|BV|0);
 //   pass 2 (all CTAs): the arcs between live vertices, as (i << 16) | j,
 //          into a work queue;
 //   then one CTA loads them into shared memory and peels SCCs by colour
@@ -1100,7 +1152,7 @@ __device__ bool res_extract(Ex &ex, const Graph &g, const Work &w, Carry &cy)
     const uint32_t *L = w.L[cy.lsel];
     const uint32_t n = cy.nL;
     if (!run_pass(ex, PH_RES_TAG, [&](unsigned, unsigned) {
-            for (uint32_t i = ex.tid(); i < n; i += ex.nthr()) w.st[L[i]] = FVB | BVB | i;
+            for (uint32_t i = ex.tid(); i < n; i += ex.nthr()) w.st[L[i]] = FVB | BVB | (i + 1u);
         }))
         return false;
     const bool ok = run_pass(ex, PH_RES_EXTRACT, [&](unsigned, unsigned nxt) {
@@ -1115,8 +1167,9 @@ __device__ bool res_extract(Ex &ex, const Graph &g, const Work &w, Carry &cy)
                 uint32_t e = 0;
                 if (ok2) {
                     const uint32_t s = w.st[guard_id(u, g.V, ex.ctl)];
-                    hit = (s & (FVB | BVB)) == (FVB | BVB);
-                    e = (src << 16) | (s & 0xFFFFu);
+                    // live vertex i carries FV|BV|(i + 1); FV|BV|0 marks the first SCC's members
+                    hit = (s & (FVB | BVB)) == (FVB | BVB) && (s & RMASK) != 0u;
+                    e = (src << 16) | ((s & RMASK) - 1u);
                 }
                 warp_push(hit, e, eb, &ex.ctl->lc[nxt][C_BQ], RES_MAX_E, ex.ctl, 24);
             };
@@ -1275,7 +1328,7 @@ __device__ int hong_loop(Ex &ex, const Graph &g, const Work &w, Carry &cy, uint3
         if (ex.leader()) ex.ctl->outer++;
         const VList L{w.L[cy.lsel], cy.nL, 0u};
         const VList R{w.Q[0][(ex.gl & 1u) ^ 1u], cy.nR, 0u};   // written by the previous pass
-        if (!ph_bfs(ex, g, w, R, SeedRanges{}, true, -1, L, w.L[cy.lsel ^ 1u])) return RUN_ERROR;
+        if (!ph_bfs(ex, g, w, R, SeedRanges{}, true, -1, L)) return RUN_ERROR;
         if (!ph_hong_update(ex, g, w, L, w.L[cy.lsel ^ 1u], false, true)) return RUN_ERROR;
         cy.nL = last_count(ex, C_LIST);
         cy.nR = last_count(ex, C_RNG);
@@ -1329,12 +1382,11 @@ __device__ __forceinline__ unsigned long long vld64(const unsigned long long *p)
 // (scc_WCC.cu:717-743, scc_Coloring.cu:539-565; wHong / wSlota run it with
 // the virtual-warp schedule, scc_WCC.cu:209-317, scc_Coloring.cu:154-263).
 template <class Ex>
-__device__ bool first_fwbw(Ex &ex, const Graph &g, const Work &w, int lw, VList scope)
+__device__ bool first_fwbw(Ex &ex, const Graph &g, const Work &w, int lw, VList scope, VList *last = nullptr)
 {
     const unsigned long long k = vld64(&w.pivkey[0]);
     const uint32_t p = k ? key_vertex(k) : 0u;
-    // L[1] is written only by the update pass after this search
-    return ph_bfs(ex, g, w, VList{nullptr, k ? 1u : 0u, p}, SeedOne{p}, true, lw, scope, w.L[1]);
+    return ph_bfs(ex, g, w, VList{nullptr, k ? 1u : 0u, p}, SeedOne{p}, true, lw, scope, last);
 }
 
 // vHong / wHong up to the main loop (scc_WCC.cu:573-848): trim1*, first
@@ -1381,8 +1433,16 @@ __device__ int slota_front(Ex &ex, const Graph &g, const Work &w, bool t1, int l
     } else if (!ph_init(ex, g, w, true)) {
         return RUN_ERROR;
     }
-    if (!first_fwbw(ex, g, w, lw, scope)) return RUN_ERROR;
-    if (!ph_slota_first_update(ex, g, w, scope, w.L[1])) return RUN_ERROR;
+    if constexpr (Ex::nbq > 2) {
+        // whole GPU: the first SCC's members keep their FV|BV mark and the
+        // update walks only the search's final, shrunken scope
+        VList last = scope;
+        if (!first_fwbw(ex, g, w, lw, scope, &last)) return RUN_ERROR;
+        if (!ph_slota_first_update_lazy(ex, g, w, last, w.L[1])) return RUN_ERROR;
+    } else {
+        if (!first_fwbw(ex, g, w, lw, scope)) return RUN_ERROR;
+        if (!ph_slota_first_update(ex, g, w, scope, w.L[1])) return RUN_ERROR;
+    }
     cy.lsel = 1u;
     cy.nL = last_count(ex, C_LIST);
     cy.nE = last_count(ex, C_FE);
@@ -1401,7 +1461,7 @@ __device__ int slota_peels(Ex &ex, const Graph &g, const Work &w, Carry &cy, uin
         if (ex.leader()) ex.ctl->outer++;
         const VList L{w.L[cy.lsel], cy.nL, 0u};
         if (!ph_propagate<true>(ex, g, w, L)) return RUN_ERROR;
-        if (!ph_bfs(ex, g, w, L, SeedRoot{}, false, -1, L, w.L[cy.lsel ^ 1u])) return RUN_ERROR;
+        if (!ph_bfs(ex, g, w, L, SeedRoot{}, false, -1, L)) return RUN_ERROR;
         if (!ph_slota_peel_update(ex, g, w, L, w.L[cy.lsel ^ 1u])) return RUN_ERROR;
         cy.nL = last_count(ex, C_LIST);
         cy.nE = last_count(ex, C_FE);

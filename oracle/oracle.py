@@ -40,6 +40,9 @@ def _load():
             fn.restype = ctypes.c_int
             fn.argtypes = [ctypes.c_uint32, u32p, u32p, u32p, u32p,
                            ctypes.c_int, ctypes.c_int, u32p, u64p]
+        lib.oracle_detect.restype = ctypes.c_int
+        lib.oracle_detect.argtypes = [ctypes.c_uint32, u32p, u32p, u32p, u32p, u32p, ctypes.c_int, ctypes.c_int,
+                                      u64p, u32p, u32p]
         _lib = lib
     return _lib
 
@@ -104,3 +107,40 @@ def hong(V, Fr, Fc, Br, Bc, t1=True, t2=True):
 def slota(V, Fr, Fc, Br, Bc, t1=True, t2=True):
     """Restated vSlota/wSlota: (labels, [trim1, 0, pivots])."""
     return _phase(_load().oracle_slota, V, Fr, Fc, Br, Bc, t1, t2)
+
+
+DETECT_HEAD = ("LOCAL SCC's IDENTIFIED! NODES WITH SAME RANGE VALUES BELONG TO THE SAME SCC!!\n"
+               "Fs AND Bs ARE POPULATED!!\nSTARTING MERGE!\n")
+
+
+def detect(V, Fr, Fc, Br, Bc, Pr, t1=True, t2=True):
+    """Restated detectSCC (-a d): ([trim1, trim2, distinct ranges], merge rounds, "No space!" round mask)."""
+    lib = _load()
+    arrs = [np.ascontiguousarray(a, dtype=np.uint32) for a in (Fr, Fc, Br, Bc)]
+    arrs = [a if a.size else np.zeros(1, np.uint32) for a in arrs]
+    Pr = np.ascontiguousarray(Pr, dtype=np.uint32)
+    if Pr.size < V + 2:
+        Pr = np.concatenate([Pr, np.zeros(V + 2 - Pr.size, np.uint32)])
+    counts = np.zeros(3, dtype=np.uint64)
+    rounds = ctypes.c_uint32(0)
+    nospace = ctypes.c_uint32(0)
+    rc = lib.oracle_detect(V, *(_p(a) for a in arrs), _p(Pr), int(bool(t1)), int(bool(t2)),
+                           counts.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), ctypes.byref(rounds),
+                           ctypes.byref(nospace))
+    if rc == 3:
+        raise MemoryError("oracle out of memory")
+    if rc != 0:
+        raise RuntimeError("detectSCC restatement: local loop did not converge")
+    return [int(c) for c in counts], int(rounds.value), int(nospace.value)
+
+
+def detect_stdout(counts, rounds, nospace, time_text="T"):
+    """The text the reference's detectSCC prints, then main's newline (scc_WCC.cu:1264-1561, scc.cu:109)."""
+    out = DETECT_HEAD
+    for r in range(1, rounds + 1):
+        out += f"Iterations {r}\n"
+        if r <= 32 and (nospace >> (r - 1)) & 1:
+            out += "No space!\n"
+    out += "MERGING DONE! ^_^\n"
+    out += f"\nNumber Of Sccs : {sum(counts)}\nTime : {time_text}\n\n"
+    return out

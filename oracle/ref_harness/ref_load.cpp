@@ -8,9 +8,10 @@
 // header lines, read "p sp V E", read E arcs "a u v w", sort by (u, v),
 // 1-based forward CSR with Fr[0]=Fr[1]=0 and V+2 offsets, reverse CSR by
 // counting sort, *oRSize = V.  Differences, all outside the SCC path:
-//   * the METIS partition array Pr is zero-filled instead of being read from
-//     the reference's hardcoded path (load.cpp:115-130), which only the
-//     out-of-scope -a d driver uses;
+//   * the METIS partition array Pr is read from the file named by the
+//     environment variable SCC_METIS_PARTITION (one id per vertex, as
+//     load.cpp:127-131 reads it) instead of the reference's hardcoded path
+//     (load.cpp:115-130), and zero-filled without it; only -a d reads it;
 //   * files that start with the 8-byte magic "SCCBIN01" are read as the
 //     project's binary CSR (u64 V, u64 E, Fr[V+2], Fc[E], Br[V+2], Bc[E],
 //     all uint32 little-endian) so large synthetic graphs skip text parsing.
@@ -22,6 +23,22 @@
 #include <algorithm>
 #include <fstream>
 #include <utility>
+
+// Pr[1..V] from SCC_METIS_PARTITION when it is set; false if that file is
+// unreadable or short (the reference prints its message and returns).
+static bool fill_partition(uint32_t V, uint32_t *Pr)
+{
+    const char *path = getenv("SCC_METIS_PARTITION");
+    if (!path || !*path) return true;
+    std::ifstream ism(path);
+    if (!ism.is_open()) return false;
+    for (uint32_t k = 0; k < V; k++) {
+        uint32_t x;
+        if (!(ism >> x)) return false;
+        Pr[k + 1] = x;
+    }
+    return true;
+}
 
 void loadFullGraph(const char *filename, uint32_t *oCSize, uint32_t *oRSize, uint32_t **oFc,
                    uint32_t **oFr, uint32_t **oBc, uint32_t **oBr, uint32_t **oPr)
@@ -41,6 +58,7 @@ void loadFullGraph(const char *filename, uint32_t *oCSize, uint32_t *oRSize, uin
         fclose(f);
         if (!ok) { printf("Error Reading graph file\n"); return; }
         uint32_t *Pr = new uint32_t[V + 2]();
+        if (!fill_partition((uint32_t)V, Pr)) { printf("Error Reading metis graph file\n"); return; }
         *oCSize = (uint32_t)E; *oRSize = (uint32_t)V;
         *oFc = Fc; *oFr = Fr; *oBc = Bc; *oBr = Br; *oPr = Pr;
         return;
@@ -63,6 +81,7 @@ void loadFullGraph(const char *filename, uint32_t *oCSize, uint32_t *oRSize, uin
     std::vector<uint32_t> fill(Br, Br + V + 2);
     for (uint32_t k = 0; k < E; k++) Bc[fill[edges[k].second]++] = (uint32_t)edges[k].first;
     uint32_t *Pr = new uint32_t[V + 2]();
+    if (!fill_partition(V, Pr)) { printf("Error Reading metis graph file\n"); return; }
     *oCSize = E; *oRSize = V;
     *oFc = Fc; *oFr = Fr; *oBc = Bc; *oBr = Br; *oPr = Pr;
 }

@@ -508,3 +508,325 @@ int oracle_slota(uint32_t V, const uint32_t *Fr, const uint32_t *Fc,
     free_state(&s);
     return OR_OK;
 }
+
+/* ------------------------------------------------------------------ */
+/* detectSCC (-a d): sequential restatement                           */
+/* ------------------------------------------------------------------ */
+/* The reference's METIS-partitioned driver (scc_WCC.cu:1000-1561) with its
+ * kernels (scc_kernels.cu:21-55, 77-122, 144-185, 388-416, 447-475,
+ * 665-852; identifyTransEdges and VecPushBack, scc_WCC.cu:10-50), on the
+ * reference's own state: uint8 tags (scc.h:24-43) and uint32 ranges that
+ * split as 3 * range + FV + 2 * BV (wrapping), with pivots kept per
+ * (partition, range mod (V + 1)).  Its printed count is
+ *   #trim-1 tags + #trim-2 tags + #distinct range values of every other
+ *   vertex (scc_WCC.cu:1533-1546),
+ * so range values that coincide count once, and the larger member of a
+ * trim-2 pair (rangeSet, no tag, range 0) adds range 0 when no other vertex
+ * keeps it.  Deterministic where the reference races: a pivot is the
+ * largest uint32 degree product of its (partition, slot), ties to the
+ * smallest id (pollForPivotsLocal's unsynchronised max); trim-2 decides on
+ * the state before its pass.
+ *
+ * Pr: V + 2 partition ids (Pr[v] for vertex v).  counts: [trim-1, trim-2,
+ * distinct ranges].  *rounds: merge rounds ("Iterations k" lines);
+ * *nospace: bit r-1 set when round r printed "No space!".  Returns 0,
+ * OR_ERR_OOM, or 2 when the local FW-BW loop passes V + 2 iterations (the
+ * reference's loop would not end).  Fs / Bs sets are only read for the
+ * ends of cross-partition edges, so they are computed for those alone. */
+#define DT_FV 1u
+#define DT_BV 2u
+#define DT_RS 16u
+#define DT_T1 32u
+#define DT_T2 64u
+#define DT_PIV 128u
+
+typedef struct {
+    uint32_t V;
+    const uint32_t *Fr, *Fc, *Br, *Bc;
+    unsigned char *tags, *aux, *occ;
+    uint32_t *range, *Pr, *queue, *mark;
+    uint32_t gen;
+} DState;
+
+static int d_live_same(const DState *s, const uint32_t *R, const uint32_t *C, uint32_t v)
+{
+    for (uint32_t e = R[v]; e < R[v + 1]; e++) {
+        uint32_t w = C[e];
+        if (!(s->tags[w] & DT_RS) && s->range[w] == s->range[v]) return 1;
+    }
+    return 0;
+}
+
+static void d_trim1(DState *s)   /* trim1 to its fixpoint (scc_kernels.cu:187-233) */
+{
+    for (int ch = 1; ch;) {
+        ch = 0;
+        for (uint32_t v = 1; v <= s->V; v++) {
+            if (s->tags[v] & DT_RS) continue;
+            if (!d_live_same(s, s->Br, s->Bc, v) || !d_live_same(s, s->Fr, s->Fc, v)) {
+                s->tags[v] |= DT_RS | DT_T1;
+                ch = 1;
+            }
+        }
+    }
+}
+
+static uint32_t d_upto2(const DState *s, const uint32_t *R, const uint32_t *C, uint32_t x, uint32_t *first)
+{
+    uint32_t n = 0;
+    for (uint32_t e = R[x]; e < R[x + 1]; e++) {
+        uint32_t w = C[e];
+        if (!(s->tags[w] & DT_RS) && s->range[w] == s->range[x]) {
+            if (++n == 2) break;
+            if (first) *first = w;
+        }
+    }
+    return n;
+}
+
+static uint32_t d_trim2_partner(const DState *s, uint32_t v)   /* scc_kernels.cu:236-348 */
+{
+    uint32_t k = 0;
+    if (d_upto2(s, s->Br, s->Bc, v, &k) == 1)
+        for (uint32_t e = s->Fr[v]; e < s->Fr[v + 1]; e++)
+            if (s->Fc[e] == k) {
+                if (d_upto2(s, s->Br, s->Bc, k, NULL) == 1) return k;
+                break;
+            }
+    k = 0;
+    if (d_upto2(s, s->Fr, s->Fc, v, &k) == 1)
+        for (uint32_t e = s->Br[v]; e < s->Br[v + 1]; e++)
+            if (s->Bc[e] == k) {
+                if (d_upto2(s, s->Fr, s->Fc, k, NULL) == 1) return k;
+                break;
+            }
+    return 0;
+}
+
+/* Closure from x in direction (R, C) over vertices without rangeSet in x's
+ * partition (fwdRc / bwdRc, scc_kernels.cu:806-852); marks them with a new
+ * generation in s->mark and returns that generation. */
+static uint32_t d_closure(DState *s, const uint32_t *R, const uint32_t *C, uint32_t x)
+{
+    const uint32_t gen = ++s->gen;
+    uint32_t head = 0, tail = 0;
+    s->mark[x] = gen;
+    s->queue[tail++] = x;
+    while (head < tail) {
+        uint32_t u = s->queue[head++];
+        for (uint32_t e = R[u]; e < R[u + 1]; e++) {
+            uint32_t w = C[e];
+            if (s->mark[w] != gen && !(s->tags[w] & DT_RS) && s->Pr[w] == s->Pr[u]) {
+                s->mark[w] = gen;
+                s->queue[tail++] = w;
+            }
+        }
+    }
+    return gen;
+}
+
+static int d_cmp_u32(const void *a, const void *b)
+{
+    uint32_t x = *(const uint32_t *)a, y = *(const uint32_t *)b;
+    return x < y ? -1 : x > y;
+}
+
+static uint32_t d_find(uint32_t *p, uint32_t x)
+{
+    while (p[x] != x) { p[x] = p[p[x]]; x = p[x]; }
+    return x;
+}
+
+int oracle_detect(uint32_t V, const uint32_t *Fr, const uint32_t *Fc, const uint32_t *Br, const uint32_t *Bc,
+                  const uint32_t *Pr_in, int t1, int t2, uint64_t *counts, uint32_t *rounds, uint32_t *nospace)
+{
+    const uint32_t CSize = Fr[V + 1];
+    DState s;
+    memset(&s, 0, sizeof(s));
+    s.V = V; s.Fr = Fr; s.Fc = Fc; s.Br = Br; s.Bc = Bc;
+    s.tags = (unsigned char *)calloc((size_t)V + 2, 1);
+    s.aux = (unsigned char *)calloc((size_t)V + 2, 1);
+    s.occ = (unsigned char *)calloc((size_t)V + 2, 1);
+    s.range = (uint32_t *)calloc((size_t)V + 2, 4);
+    s.Pr = (uint32_t *)malloc(((size_t)V + 2) * 4);
+    s.queue = (uint32_t *)malloc(((size_t)V + 2) * 4);
+    s.mark = (uint32_t *)calloc((size_t)V + 2, 4);
+    uint32_t maxp = 0;
+    for (uint32_t v = 1; v <= V; v++) maxp = Pr_in[v] > maxp ? Pr_in[v] : maxp;
+    const size_t nslot = ((size_t)maxp + 1) * ((size_t)V + 1);
+    uint32_t *best_v = (uint32_t *)malloc(nslot * 4), *best_p = (uint32_t *)malloc(nslot * 4);
+    uint32_t *dsu = (uint32_t *)malloc(((size_t)V + 2) * 4), *rmax = (uint32_t *)malloc(((size_t)V + 2) * 4);
+    uint32_t *Rm = (uint32_t *)malloc(((size_t)maxp + 2) * 4);
+    uint32_t *tu = (uint32_t *)malloc(10001 * 4), *tv = (uint32_t *)malloc(10001 * 4);
+    int rc = OR_OK;
+    if (!s.tags || !s.aux || !s.occ || !s.range || !s.Pr || !s.queue || !s.mark || !best_v || !best_p || !dsu ||
+        !rmax || !Rm || !tu || !tv) { rc = OR_ERR_OOM; goto out; }
+    memcpy(s.Pr, Pr_in, ((size_t)V + 2) * 4);
+    s.tags[0] = DT_RS;
+    /* trims (scc_WCC.cu:1123-1175) */
+    if (t1) d_trim1(&s);
+    if (t2) {
+        uint32_t n = 0;
+        for (uint32_t v = 1; v <= V; v++) {
+            if (s.tags[v] & DT_RS) continue;
+            uint32_t k = d_trim2_partner(&s, v);
+            if (k) { s.queue[n++] = v; s.mark[v] = k; }
+        }
+        for (uint32_t i = 0; i < n; i++) {
+            uint32_t v = s.queue[i], k = s.mark[v];
+            s.tags[v] |= DT_RS;
+            s.tags[k] |= DT_RS;
+            s.tags[v < k ? v : k] |= DT_T2;
+        }
+        for (uint32_t i = 0; i < n; i++) s.mark[s.queue[i]] = 0;
+    }
+    if (t1) d_trim1(&s);
+    /* local FW-BW inside (partition, range) (scc_WCC.cu:1183-1262) */
+    for (uint32_t it = 0;; it++) {
+        if (it > V + 2) { rc = 2; goto out; }
+        for (size_t i = 0; i < nslot; i++) { best_v[i] = 0; best_p[i] = 0; }
+        for (uint32_t v = 1; v <= V; v++) {   /* pollForPivotsLocal */
+            if ((s.tags[v] & DT_RS) || s.aux[v]) continue;
+            size_t key = (size_t)s.Pr[v] * ((size_t)V + 1) + s.range[v] % (V + 1);
+            uint32_t prod = (Fr[v + 1] - Fr[v]) * (Br[v + 1] - Br[v]);
+            if (prod > best_p[key]) { best_p[key] = prod; best_v[key] = v; }
+        }
+        for (uint32_t v = 1; v <= V; v++) {   /* selectPivotsLocal */
+            if ((s.tags[v] & DT_RS) || s.aux[v]) continue;
+            size_t key = (size_t)s.Pr[v] * ((size_t)V + 1) + s.range[v] % (V + 1);
+            if (best_v[key] == v) s.tags[v] = DT_FV | DT_BV | DT_PIV;
+        }
+        for (int dir = 0; dir < 2; dir++) {   /* fwdLocal / bwdLocal to closure */
+            const uint32_t *R = dir ? Br : Fr, *C = dir ? Bc : Fc;
+            const unsigned char bit = dir ? DT_BV : DT_FV;
+            uint32_t head = 0, tail = 0;
+            for (uint32_t v = 1; v <= V; v++)
+                if (!(s.tags[v] & DT_RS) && !s.aux[v] && (s.tags[v] & bit)) s.queue[tail++] = v;
+            while (head < tail) {
+                uint32_t u = s.queue[head++];
+                for (uint32_t e = R[u]; e < R[u + 1]; e++) {
+                    uint32_t w = C[e];
+                    if ((s.tags[w] & (DT_RS | bit)) || s.aux[w] || s.range[w] != s.range[u] || s.Pr[w] != s.Pr[u]) continue;
+                    s.tags[w] |= bit;
+                    s.queue[tail++] = w;
+                }
+            }
+        }
+        int ch = 0;   /* updateLocal */
+        for (uint32_t v = 1; v <= V; v++) {
+            if ((s.tags[v] & DT_RS) || s.aux[v]) continue;
+            uint32_t f = (s.tags[v] & DT_FV) ? 1u : 0u, b = (s.tags[v] & DT_BV) ? 1u : 0u;
+            if (f && b) s.aux[v] = 1;
+            else { ch = 1; s.range[v] = 3u * s.range[v] + f + 2u * b; s.tags[v] = 0; }
+        }
+        if (!ch) break;
+    }
+    for (uint32_t v = 1; v <= V; v++)   /* resetTag over every vertex (scc_WCC.cu:1276-1333) */
+        if (!(s.tags[v] & DT_RS)) s.tags[v] = 0;
+    /* merge rounds (scc_WCC.cu:1347-1514) */
+    *rounds = 0;
+    *nospace = 0;
+    for (;;) {
+        uint32_t r = ++*rounds;
+        for (uint32_t v = 0; v <= V; v++) s.occ[v] = 0;
+        for (int dir = 0; dir < 2; dir++) {   /* computeInDegree, then computeOutDegree */
+            const uint32_t *R = dir ? Fr : Br, *C = dir ? Fc : Bc;
+            for (int ch = 1; ch;) {
+                ch = 0;
+                for (uint32_t v = 1; v <= V; v++) {
+                    if ((s.tags[v] & DT_RS) || s.occ[v]) { s.occ[v] = 1; continue; }
+                    uint32_t fr = (s.Pr[v] & 1u) ? s.Pr[v] - 1u : s.Pr[v] + 1u, deg = 0;
+                    for (uint32_t e = R[v]; e < R[v + 1]; e++) {
+                        uint32_t w = C[e];
+                        if (s.occ[w] || (s.tags[w] & DT_RS)) continue;
+                        if (s.Pr[w] == s.Pr[v] || s.Pr[w] == fr) deg++;
+                    }
+                    if (!deg) { s.occ[v] = 1; ch = 1; }
+                }
+            }
+        }
+        for (uint32_t p = 0; p <= maxp + 1; p++) Rm[p] = 0;   /* getMaxRange, shiftRange */
+        for (uint32_t v = 1; v <= V; v++)
+            if (!(s.tags[v] & DT_RS) && !(s.Pr[v] & 1u) && s.range[v] > Rm[s.Pr[v]]) Rm[s.Pr[v]] = s.range[v];
+        for (uint32_t v = 1; v <= V; v++)
+            if (!(s.tags[v] & DT_RS) && (s.Pr[v] & 1u)) s.range[v] = s.range[v] + Rm[s.Pr[v] - 1u] + 1u;
+        uint32_t nt = 0, dsize = 0;   /* identifyTransEdges: at most 10001 kept (VecPushBack) */
+        for (uint32_t v = 1; v <= V; v++) {
+            if ((s.tags[v] & DT_RS) || s.occ[v]) continue;
+            uint32_t fr = (s.Pr[v] & 1u) ? s.Pr[v] - 1u : s.Pr[v] + 1u;
+            for (uint32_t e = Fr[v]; e < Fr[v + 1]; e++) {
+                uint32_t w = Fc[e];
+                if (!(s.tags[w] & DT_RS) && s.Pr[w] == fr && !s.occ[w]) {
+                    if (dsize < 10001) { tu[nt] = v; tv[nt] = w; nt++; }
+                    dsize++;
+                }
+            }
+        }
+        if (dsize >= CSize && r <= 32) *nospace |= 1u << (r - 1);
+        if (dsize > 10001) nt = 0;   /* the reference's copy of dsize entries from a 10001-entry array fails */
+        /* trans sets: Bs[u1_i] & Fs[u2_j] joined with Bs[u1_j] & Fs[u2_i] for every pair i < j
+         * (scc_WCC.cu:1400-1433); the members of a non-empty set end with the largest range of the
+         * sets they are joined through (the fixpoint of :1442-1462), i.e. the largest range of their
+         * component when every set joins its members */
+        for (uint32_t v = 0; v <= V; v++) dsu[v] = v;
+        if (nt > 1) {
+            const size_t W = ((size_t)V + 64) / 64;
+            uint64_t *Fs = (uint64_t *)calloc((size_t)nt * W, 8), *Bs = (uint64_t *)calloc((size_t)nt * W, 8);
+            if (!Fs || !Bs) { free(Fs); free(Bs); rc = OR_ERR_OOM; goto out; }
+            for (uint32_t i = 0; i < nt; i++) {   /* Fs of the targets, Bs of the sources */
+                uint32_t g = d_closure(&s, Fr, Fc, tv[i]);
+                for (uint32_t v = 1; v <= V; v++) if (s.mark[v] == g) Fs[i * W + v / 64] |= 1ull << (v % 64);
+                g = d_closure(&s, Br, Bc, tu[i]);
+                for (uint32_t v = 1; v <= V; v++) if (s.mark[v] == g) Bs[i * W + v / 64] |= 1ull << (v % 64);
+            }
+            for (uint32_t i = 0; i < nt; i++)
+                for (uint32_t j = i + 1; j < nt; j++) {
+                    uint32_t rep = 0;
+                    for (int side = 0; side < 2; side++) {
+                        const uint64_t *x = Bs + (size_t)(side ? j : i) * W, *y = Fs + (size_t)(side ? i : j) * W;
+                        for (size_t k = 0; k < W; k++) {
+                            uint64_t m = x[k] & y[k];
+                            while (m) {
+                                uint32_t v = (uint32_t)(k * 64 + (uint32_t)__builtin_ctzll(m));
+                                m &= m - 1;
+                                if (!rep) rep = v;
+                                else dsu[d_find(dsu, v)] = d_find(dsu, rep);
+                            }
+                        }
+                    }
+                }
+            free(Fs);
+            free(Bs);
+        }
+        for (uint32_t v = 1; v <= V; v++) rmax[v] = s.range[v];
+        for (uint32_t v = 1; v <= V; v++) {
+            uint32_t root = d_find(dsu, v);
+            if (rmax[root] < s.range[v]) rmax[root] = s.range[v];
+        }
+        for (uint32_t v = 1; v <= V; v++) s.range[v] = rmax[d_find(dsu, v)];
+        int more = 0;   /* updatePr */
+        for (uint32_t v = 1; v <= V; v++) {
+            if (s.tags[v] & DT_RS) continue;
+            if (s.Pr[v] & 1u) { s.Pr[v] -= 1u; more = 1; }
+            s.Pr[v] >>= 1;
+        }
+        if (!more) break;
+    }
+    {   /* the count (scc_WCC.cu:1533-1546) */
+        uint64_t n1 = 0, n2 = 0, np = 0;
+        uint32_t ns = 0;
+        for (uint32_t v = 1; v <= V; v++) {
+            if (s.tags[v] & DT_T1) n1++;
+            else if (s.tags[v] & DT_T2) n2++;
+            else s.queue[ns++] = s.range[v];
+        }
+        /* distinct values among the rest */
+        qsort(s.queue, ns, sizeof(uint32_t), d_cmp_u32);
+        for (uint32_t i = 0; i < ns; i++) np += (i == 0 || s.queue[i] != s.queue[i - 1]) ? 1u : 0u;
+        counts[0] = n1; counts[1] = n2; counts[2] = np;
+    }
+out:
+    free(s.tags); free(s.aux); free(s.occ); free(s.range); free(s.Pr); free(s.queue); free(s.mark);
+    free(best_v); free(best_p); free(dsu); free(rmax); free(Rm); free(tu); free(tv);
+    return rc;
+}

@@ -127,3 +127,28 @@ def test_oracle_counts_match_recorded_reference_outputs(golden, oracle_lib):
             assert r["num_sccs"] == sum(c), key
         if algo == "g" and not t2:
             assert r["numberOf1Sccs"] == c[0], key
+
+
+def test_detect_restatement_matches_reference_binary_outputs(oracle_lib, golden):
+    """The restated detectSCC (-a d) prints exactly what the reference
+    binary printed on the shipped samples with their shipped METIS
+    partitions and with none (tests/golden/ref_detect.json, recorded on a
+    B200 by tests/golden/make_ref_detect.py; time value masked), including
+    the case where its range arithmetic over-counts (sample128, -q 1)."""
+    import json
+    import os
+    from conftest import GOLDEN
+    rec = json.load(open(os.path.join(GOLDEN, "ref_detect.json")))
+    parts = np.load(os.path.join(GOLDEN, "metis_partitions.npz"))
+    assert len(rec) >= 20
+    for key, r in rec.items():
+        name, part, q = key.split(":")
+        z = golden[name]
+        V = int(z["V"])
+        Fr, Fc, Br, Bc = build_csr(V, z["src"].astype(np.int64), z["dst"].astype(np.int64))
+        Pr = np.zeros(V + 2, np.uint32)
+        if part != "none":
+            Pr[1:V + 1] = parts[part][:V]
+        counts, rounds, nospace = oracle_lib.detect(V, Fr, Fc, Br, Bc, Pr, True, q == "q1")
+        assert r["stable"]
+        assert oracle_lib.detect_stdout(counts, rounds, nospace) == r["runs"][0]["stdout"], key
