@@ -149,6 +149,19 @@ class Engine:
         return Result(out[:g.V] if labels else None, st.num_sccs, st.num_trim1, st.num_trim2,
                       st.num_pivot, st.as_dict())
 
+    def detect(self, g: Graph, Pr=None, t1=True, t2=True) -> dict:
+        """detectSCC (-a d, scc_WCC.cu:1000-1617) on a host graph with METIS
+        partition ids Pr (V+2 entries, Pr[v] for vertex v; None: one partition).
+        Returns the reference's printed count and its parts."""
+        P = np.zeros(g.V + 2, dtype=np.uint32) if Pr is None else np.ascontiguousarray(Pr, dtype=np.uint32)
+        if P.shape[0] < g.V + 2:
+            raise ValueError("Pr needs V + 2 entries")
+        view = N.CsrView(g.V, g.E, _ptr(g.Fr), _ptr(g.Fc), _ptr(g.Br), _ptr(g.Bc))
+        r = N.DetectResult()
+        flags = (N.FLAG_TRIM1 if t1 else 0) | (N.FLAG_TRIM2 if t2 else 0)
+        N.check(self._lib.scc_detect(self._h, ctypes.byref(view), _ptr(P), flags, ctypes.byref(r)), "scc_detect")
+        return {k: getattr(r, k) for k, _ in N.DetectResult._fields_}
+
     def derive_reverse(self, V: int, E: int, Fr, Fc, Br, Bc, stream=None) -> None:
         """Fill device arrays Br (V+2) and Bc (E) with the reverse CSR of (Fr, Fc)."""
         if stream is None and hasattr(Fr, "device") and getattr(Fr.device, "type", "") == "cuda":

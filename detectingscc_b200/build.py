@@ -33,7 +33,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-Wall", "-I/usr/local/cuda/include"]
 
-CU_SOURCES = ["scc_engine.cu", "scc_batch.cu", "scc_noalloc.cu", "scc_serve.cu", "scc_transpose.cu"]
+CU_SOURCES = ["scc_engine.cu", "scc_batch.cu", "scc_noalloc.cu", "scc_serve.cu", "scc_transpose.cu", "scc_detect.cu"]
 CXX_LIB_SOURCES = ["gtgraph_load.cpp", "scc_compat.cpp"]
 CXX_CLI_SOURCES = ["scc_cli.cpp", "scc_metis_cli.cpp"]
 HEADERS = ["scc_device.cuh", "scc_phases.cuh", "scc_internal.h", "scc_host.h", "scc_batch_internal.h"]

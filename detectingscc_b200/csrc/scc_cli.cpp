@@ -62,11 +62,7 @@ int main(int argc, char **argv)
         default: print_help(); return 1;
         }
     }
-    if (algo == 'd') {
-        fprintf(stderr, "scc: -a d (detectSCC) is not provided by this engine\n");
-        return 1;
-    }
-    if (algo != 'g' && algo != 'h' && algo != 'x' && algo != 'y') {
+    if (algo != 'g' && algo != 'h' && algo != 'x' && algo != 'y' && algo != 'd') {
         print_help();
         return 1;
     }
@@ -86,6 +82,7 @@ int main(int argc, char **argv)
         case 'h': vSlota(CSize, RSize, Fc, Fr, Bc, Br, trim1, trim2); break;
         case 'x': wHong(CSize, RSize, Fc, Fr, Bc, Br, trim1, trim2, warpSize); break;
         case 'y': wSlota(CSize, RSize, Fc, Fr, Bc, Br, trim1, trim2, warpSize); break;
+        case 'd': detectSCC(CSize, RSize, Fc, Fr, Bc, Br, Pr, trim1, trim2); break;
         }
     } catch (const char *e) {
         printf("%s\n", e);
@@ -94,7 +91,7 @@ int main(int argc, char **argv)
     printf("\n");
     fflush(stdout);
 
-    if (labels_path || json) {
+    if ((labels_path || json) && algo != 'd') {
         scc_context *ctx = nullptr;
         int rc = scc_create(getenv("SCC_DEVICE") ? atoi(getenv("SCC_DEVICE")) : 0, &ctx);
         uint32_t *labels = labels_path ? new uint32_t[RSize ? RSize : 1] : nullptr;

@@ -89,12 +89,41 @@ void wSlota(uint32_t CSize, uint32_t RSize, uint32_t *Fc, uint32_t *Fr, uint32_t
     run_or_die(SCC_ALGO_WSLOTA, CSize, RSize, Fc, Fr, Bc, Br, t1, t2, warpSize);
 }
 
-// detectSCC (scc.h:53, scc_WCC.cu:1000-1617) -- the METIS-partitioned
-// experiment -- is not provided.  The symbol exists so that the reference's
-// own scc.cu links unchanged; calling it throws a const char*, which the
-// reference's main catches, prints and turns into exit status 1
-// (scc.cu:104-108).
-void detectSCC(uint32_t, uint32_t, uint32_t *, uint32_t *, uint32_t *, uint32_t *, uint32_t *, bool, bool)
+extern "C" int scc_reference_detect(uint32_t CSize, uint32_t RSize, const uint32_t *Fc, const uint32_t *Fr,
+                                    const uint32_t *Bc, const uint32_t *Br, const uint32_t *Pr, int t1, int t2,
+                                    uint64_t *num_sccs_out)
 {
-    throw "detectSCC (-a d) is not provided by this engine";
+    auto t0 = std::chrono::steady_clock::now();
+    int status = SCC_OK;
+    scc_context *ctx = shared_context(&status);
+    if (!ctx) return status;
+    scc_csr_view g{RSize, CSize, Fr, Fc, Br, Bc};
+    scc_detect_result r;
+    const int rc = scc_detect(ctx, &g, Pr, (t1 ? SCC_FLAG_TRIM1 : 0u) | (t2 ? SCC_FLAG_TRIM2 : 0u), &r);
+    if (rc != SCC_OK) return rc;
+    printf("LOCAL SCC's IDENTIFIED! NODES WITH SAME RANGE VALUES BELONG TO THE SAME SCC!!\n");
+    printf("Fs AND Bs ARE POPULATED!!\n");
+    printf("STARTING MERGE!\n");
+    for (uint32_t k = 1; k <= r.merge_rounds; k++) {
+        printf("Iterations %u\n", k);
+        if (k <= 32 && ((r.nospace_mask >> (k - 1)) & 1u)) printf("No space!\n");
+    }
+    printf("MERGING DONE! ^_^\n");
+    const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    printf("\nNumber Of Sccs : %d", (int)r.num_sccs);
+    printf("\nTime : %f\n", ms);
+    if (num_sccs_out) *num_sccs_out = r.num_sccs;
+    return SCC_OK;
+}
+
+// detectSCC (scc.h:53, scc_WCC.cu:1000-1617), the METIS-partitioned
+// driver: same stdout, same error policy as the other shims.
+void detectSCC(uint32_t CSize, uint32_t RSize, uint32_t *Fc, uint32_t *Fr, uint32_t *Bc, uint32_t *Br, uint32_t *Pr,
+               bool t1, bool t2)
+{
+    int rc = scc_reference_detect(CSize, RSize, Fc, Fr, Bc, Br, Pr, t1, t2, nullptr);
+    if (rc == SCC_OK) return;
+    if (rc == SCC_ERR_OOM) throw "Error: Not enough memory on GPU\n";
+    fprintf(stderr, "GPUassert: %s %s %d\n", scc_status_string(rc), __FILE__, __LINE__);
+    exit(rc);
 }

@@ -274,6 +274,31 @@ int scc_save_metis(const char *path, const scc_host_graph *g);
  * 0.  Pr must hold V+2 entries. */
 int scc_load_partition(const char *path, uint32_t V, uint32_t *Pr);
 
+/* ---- detectSCC (-a d) -------------------------------------------------- */
+/* The reference's METIS-partitioned driver (scc_WCC.cu:1000-1617): SCCs
+ * inside every partition (Pr[v], V + 2 entries, host), then pairwise merges
+ * of partitions 2k and 2k+1 through the edges that cross them, with the
+ * reference's own range arithmetic.  num_sccs is what the reference prints
+ * (trim-1 tags + trim-2 tags + distinct range values of the other vertices),
+ * which is not always the number of SCCs: values that coincide count once.
+ * Host CSR only; flags: SCC_FLAG_TRIM1, SCC_FLAG_TRIM2.  Partition ids may
+ * be any uint32 (the reference indexes 10 fixed pivot tables with them,
+ * scc_WCC.cu:1035).  The merge tests every pair of crossing edges, as the
+ * reference does: meant for the small graphs that driver was written for. */
+typedef struct {
+    uint64_t num_sccs;      /* the reference's "Number Of Sccs" */
+    uint64_t num_trim1, num_trim2, num_ranges;
+    uint32_t merge_rounds;  /* the reference's "Iterations k" lines */
+    uint32_t nospace_mask;  /* bit r-1: round r printed "No space!" */
+} scc_detect_result;
+int scc_detect(scc_context *ctx, const scc_csr_view *host_graph, const uint32_t *Pr, uint32_t flags,
+               scc_detect_result *out);
+/* detectSCC with the reference's stdout (scc_WCC.cu:1264-1561): its progress
+ * lines, "Iterations k" per merge round, then "\nNumber Of Sccs : N" and
+ * "\nTime : T\n".  The C++ shim detectSCC (include/scc_compat.h) calls it. */
+int scc_reference_detect(uint32_t CSize, uint32_t RSize, const uint32_t *Fc, const uint32_t *Fr, const uint32_t *Bc,
+                         const uint32_t *Br, const uint32_t *Pr, int t1, int t2, uint64_t *num_sccs_out);
+
 /* ---- reference-compatible driver call ----------------------------------- */
 /* Runs one of the reference drivers with its exact stdout: for 'g' the line
  * "numberOf1Sccs: N\n", then "\nNumber Of Sccs : N" and "\nTime : T" (ms,

@@ -21,9 +21,18 @@ def test_too_few_arguments_prints_help(native):
     assert r.returncode == 1 and r.stdout == HELP
 
 
-def test_detect_scc_is_not_provided(native, tmp_path):
+def test_detect_scc_reads_its_graph_and_partition_first(native, tmp_path, monkeypatch):
+    # -a d (detectSCC) loads the graph, then the METIS partition named by
+    # SCC_METIS_PARTITION; a file that cannot be read is reported before any
+    # device work, with the reference's messages (load.cpp:24-28, :119-123)
     r = _run(native, "-a", "d", "-p", "1", "-q", "1", "-w", "1", "-f", str(tmp_path / "x.gr"))
-    assert r.returncode == 1 and "detectSCC" in r.stderr
+    assert r.returncode == 1 and r.stdout.startswith("Error Reading graph file")
+    from oracle.gtgraph_ref import write_gtgraph
+    gr = str(tmp_path / "g.gr")
+    write_gtgraph(gr, 3, [1, 2], [2, 3], "g")
+    monkeypatch.setenv("SCC_METIS_PARTITION", str(tmp_path / "missing.part"))
+    r = _run(native, "-a", "d", "-p", "1", "-q", "1", "-w", "1", "-f", gr)
+    assert r.returncode == 1 and r.stdout.startswith("Error Reading metis graph file")
 
 
 def test_bad_warp_width_rejected(native, tmp_path):
