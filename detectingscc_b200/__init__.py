@@ -8,8 +8,9 @@ call raises ``NativeLibraryError``.
 """
 from ._native import NativeLibraryError, SCCError  # noqa: F401
 from .api import (ALGOS, Batch, Engine, Graph, Result, Server, graph_from_arcs, load_graph,  # noqa: F401
-                  load_partition, loadFullGraph, save_binary, save_metis, vHong, vSlota, wHong, wSlota)
+                  load_partition, loadFullGraph, save_binary, save_gtgraph, save_metis, vHong, vSlota, wHong,
+                  wSlota)
 
 __all__ = ["Batch", "Engine", "Server", "Graph", "Result", "graph_from_arcs", "load_graph", "loadFullGraph",
-           "save_binary", "save_metis", "load_partition", "vHong", "vSlota", "wHong", "wSlota", "NativeLibraryError", "SCCError",
+           "save_binary", "save_gtgraph", "save_metis", "load_partition", "vHong", "vSlota", "wHong", "wSlota", "NativeLibraryError", "SCCError",
            "ALGOS"]

@@ -87,7 +87,7 @@ MAX_VERTICES = 268435454
 # every symbol include/scc_b200.h and include/scc_compat.h declare
 C_SYMBOLS = ["scc_create", "scc_destroy", "scc_run", "scc_set_tuning", "scc_status_string",
              "scc_version", "scc_get_trace", "scc_derive_reverse", "scc_load_graph", "scc_save_binary", "scc_graph_from_arcs",
-             "scc_free_host_graph", "scc_save_metis", "scc_load_partition", "scc_detect", "scc_reference_detect",
+             "scc_free_host_graph", "scc_save_gtgraph", "scc_load_graph_device", "scc_save_metis", "scc_load_partition", "scc_detect", "scc_reference_detect",
              "scc_reference_call", "scc_batch_create", "scc_batch_run",
              "scc_batch_destroy", "scc_run_noalloc", "scc_batch_set_schedule", "scc_batch_get_schedule",
              "scc_batch_autotune", "scc_batch_info", "scc_batch_set_cluster", "scc_batch_get_cluster", "scc_server_create", "scc_server_submit",
@@ -131,6 +131,8 @@ def lib():
     L.scc_save_binary.argtypes = [ctypes.c_char_p, ctypes.POINTER(HostGraph)]
     L.scc_graph_from_arcs.argtypes = [u32, u64, vp, vp, ctypes.POINTER(HostGraph)]
     L.scc_save_metis.argtypes = [ctypes.c_char_p, ctypes.POINTER(HostGraph)]
+    L.scc_save_gtgraph.argtypes = [ctypes.c_char_p, ctypes.POINTER(HostGraph)]
+    L.scc_load_graph_device.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(CsrView), vp]
     L.scc_detect.argtypes = [vp, ctypes.POINTER(CsrView), vp, u32, ctypes.POINTER(DetectResult)]
     L.scc_reference_detect.argtypes = [u32, u32, vp, vp, vp, vp, vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(u64)]
     L.scc_load_partition.argtypes = [ctypes.c_char_p, u32, vp]

@@ -162,6 +162,16 @@ class Engine:
         N.check(self._lib.scc_detect(self._h, ctypes.byref(view), _ptr(P), flags, ctypes.byref(r)), "scc_detect")
         return {k: getattr(r, k) for k, _ in N.DetectResult._fields_}
 
+    def load_graph_device(self, path: str, stream=None):
+        """Parse a GTgraph file (or the binary CSR format) on the device and build
+        both CSRs there.  Returns (V, E, Fr, Fc, Br, Bc) with device pointers
+        (ints) into this engine's CSR arrays, for run_device; they stay valid
+        until the next load or run with host inputs on this engine."""
+        view = N.CsrView()
+        N.check(self._lib.scc_load_graph_device(self._h, path.encode(), ctypes.byref(view), stream),
+                f"scc_load_graph_device({path})")
+        return view.num_vertices, view.num_edges, view.Fr, view.Fc, view.Br, view.Bc
+
     def derive_reverse(self, V: int, E: int, Fr, Fc, Br, Bc, stream=None) -> None:
         """Fill device arrays Br (V+2) and Bc (E) with the reverse CSR of (Fr, Fc)."""
         if stream is None and hasattr(Fr, "device") and getattr(Fr.device, "type", "") == "cuda":
@@ -369,6 +379,13 @@ def save_binary(path: str, g: Graph) -> None:
     hg = N.HostGraph(g.V, g.E, g.Fr.ctypes.data_as(N.u32p), g.Fc.ctypes.data_as(N.u32p),
                      g.Br.ctypes.data_as(N.u32p), g.Bc.ctypes.data_as(N.u32p), None)
     N.check(N.lib().scc_save_binary(path.encode(), ctypes.byref(hg)), f"save {path}")
+
+
+def save_gtgraph(path: str, g: Graph) -> None:
+    """Write g as GTgraph text (the reference's input format, load.cpp:12-45)."""
+    hg = N.HostGraph(g.V, g.E, g.Fr.ctypes.data_as(N.u32p), g.Fc.ctypes.data_as(N.u32p),
+                     g.Br.ctypes.data_as(N.u32p), g.Bc.ctypes.data_as(N.u32p), None)
+    N.check(N.lib().scc_save_gtgraph(path.encode(), ctypes.byref(hg)), f"save {path}")
 
 
 def save_metis(path: str, g: Graph) -> None:

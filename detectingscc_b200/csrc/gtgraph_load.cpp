@@ -276,6 +276,46 @@ extern "C" int scc_save_metis(const char *path, const scc_host_graph *g)
     return ok ? SCC_OK : SCC_ERR_IO;
 }
 
+// GTgraph text: the seven comment lines the reference skips, "p sp V E",
+// then "a u v 1" per arc in forward order.
+extern "C" int scc_save_gtgraph(const char *path, const scc_host_graph *g)
+{
+    if (!path || !g || (g->V && !g->Fr) || (g->E && !g->Fc)) return SCC_ERR_INVALID_ARG;
+    FILE *f = fopen(path, "wb");
+    if (!f) return SCC_ERR_IO;
+    const size_t cap = 4u << 20;
+    std::vector<char> buf;
+    try {
+        buf.resize(cap + 128);
+    } catch (...) {
+        fclose(f);
+        return SCC_ERR_OOM;
+    }
+    char *o = buf.data();
+    bool ok = true;
+    o += snprintf(o, 128, "c FILE\t\t\t: graph\nc No. of vertices\t: %u\nc No. of directed edges\t: %u\n", g->V, g->E);
+    ok = ok && fwrite(buf.data(), 1, (size_t)(o - buf.data()), f) == (size_t)(o - buf.data());
+    o = buf.data();
+    o += snprintf(o, 128, "c Max. weight\t\t: 1\nc Min. weight\t\t: 1\nc A directed arc from u to v of weight w\n");
+    o += snprintf(o, 128, "c is represented below as ' a  u  v  w '\np sp %u %u\n", g->V, g->E);
+    for (uint32_t u = 1; u <= g->V; u++)
+        for (uint32_t e = g->Fr[u]; e < g->Fr[u + 1]; e++) {
+            *o++ = 'a';
+            *o++ = ' ';
+            o = put_u32_sp(o, u);
+            o = put_u32_sp(o, g->Fc[e]);
+            *o++ = '1';
+            *o++ = '\n';
+            if ((size_t)(o - buf.data()) >= cap) {
+                ok = ok && fwrite(buf.data(), 1, (size_t)(o - buf.data()), f) == (size_t)(o - buf.data());
+                o = buf.data();
+            }
+        }
+    ok = ok && fwrite(buf.data(), 1, (size_t)(o - buf.data()), f) == (size_t)(o - buf.data());
+    ok = (fclose(f) == 0) && ok;
+    return ok ? SCC_OK : SCC_ERR_IO;
+}
+
 // One partition id per vertex, whitespace separated (load.cpp:127-131).
 extern "C" int scc_load_partition(const char *path, uint32_t V, uint32_t *Pr)
 {

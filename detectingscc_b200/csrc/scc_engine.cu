@@ -268,7 +268,7 @@ int scc_ctx_reserve(scc_context *ctx, uint32_t V, uint32_t E)
     return SCC_OK;
 }
 
-static int ensure_csr_mirror(scc_context *ctx, uint32_t V, uint32_t E)
+int sccb_csr_mirror(scc_context *ctx, uint32_t V, uint32_t E)
 {
     size_t nv = (size_t)V + 2, ne = std::max<size_t>(E, 1);
     if (nv > ctx->capV) {
@@ -344,13 +344,17 @@ extern "C" int scc_destroy(scc_context *ctx)
     if (!ctx) return SCC_ERR_INVALID_ARG;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->up) cudaStreamSynchronize(ctx->up);
     cudaFree(ctx->ws);
     cudaFree(ctx->dFr); cudaFree(ctx->dFc); cudaFree(ctx->dBr); cudaFree(ctx->dBc); cudaFree(ctx->dlab);
-    cudaFree(ctx->tsrc); cudaFree(ctx->tkey); cudaFree(ctx->ttmp); cudaFree(ctx->tctl);
+    for (auto *p : ctx->tarc) cudaFree(p);
+    cudaFree(ctx->ttmp); cudaFree(ctx->tctl); cudaFree(ctx->dtext);
     if (ctx->hctl) cudaFreeHost(ctx->hctl);
     cudaFree(ctx->dtrace);
     if (ctx->htrace) cudaFreeHost(ctx->htrace);
     for (int i = 0; i < 4; i++) if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
+    for (auto e : ctx->upev) if (e) cudaEventDestroy(e);
+    if (ctx->up) cudaStreamDestroy(ctx->up);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return SCC_OK;
@@ -446,15 +450,15 @@ extern "C" int scc_run(scc_context *ctx, const scc_csr_view *gv, int algo, uint3
     Graph g{V, E, gv->Fr, gv->Fc, gv->Br, gv->Bc, 0u};
     uint32_t *dout = labels_out;
     if (!dev || derive) {
-        rc = ensure_csr_mirror(ctx, V, E);
+        rc = sccb_csr_mirror(ctx, V, E);
         if (rc != SCC_OK) return rc;
     }
     if (!dev) {
         CK(cudaMemcpyAsync(ctx->dFr, gv->Fr, ((size_t)V + 2) * 4, cudaMemcpyHostToDevice, st));
         if (!derive) CK(cudaMemcpyAsync(ctx->dBr, gv->Br, ((size_t)V + 2) * 4, cudaMemcpyHostToDevice, st));
-        if (E) {
+        if (E && !derive) {   // with derive, Fc crosses inside sccb_derive_reverse, beside its first kernels
             CK(cudaMemcpyAsync(ctx->dFc, gv->Fc, (size_t)E * 4, cudaMemcpyHostToDevice, st));
-            if (!derive) CK(cudaMemcpyAsync(ctx->dBc, gv->Bc, (size_t)E * 4, cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(ctx->dBc, gv->Bc, (size_t)E * 4, cudaMemcpyHostToDevice, st));
         }
         g.Fr = ctx->dFr; g.Fc = ctx->dFc; g.Br = ctx->dBr; g.Bc = ctx->dBc;
         dout = labels_out ? ctx->dlab : nullptr;
@@ -474,7 +478,7 @@ extern "C" int scc_run(scc_context *ctx, const scc_csr_view *gv, int algo, uint3
     if (derive) {
         // after the control block is zeroed: input errors found here stop the SCC kernel at its entry
         rc = sccb_derive_reverse(ctx, g.Fr, g.Fc, V, E, const_cast<uint32_t *>(g.Br), const_cast<uint32_t *>(g.Bc),
-                                 ctx->work.ctl, st);
+                                 ctx->work.ctl, st, dev ? nullptr : gv->Fc);
         if (rc != SCC_OK) return rc;
     }
     CK(cudaMemsetAsync(ctx->work.pivkey, 0, hong ? (4 * ((size_t)V + 1) + 8) * 8 : 8, st));

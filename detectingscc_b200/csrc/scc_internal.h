@@ -7,6 +7,8 @@
 
 #include "scc_device.cuh"
 
+constexpr unsigned UPLOAD_CHUNKS = 8;   // pieces of a host-to-device upload beside the reverse build
+
 struct scc_context {
     int device = 0;
     int nsm = 0;
@@ -14,6 +16,9 @@ struct scc_context {
     int last_cuda_error = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    // upload of the forward targets beside the reverse-CSR build
+    cudaStream_t up = nullptr;
+    cudaEvent_t upev[UPLOAD_CHUNKS + 1] = {};
     sccb::Ctl *hctl = nullptr;   // pinned copy of the control block
 
     // device workspace (grows to the largest graph run so far)
@@ -25,12 +30,14 @@ struct scc_context {
     uint32_t *dFr = nullptr, *dFc = nullptr, *dBr = nullptr, *dBc = nullptr, *dlab = nullptr;
     size_t capV = 0, capE = 0;
 
-    // reverse CSR built on the device (SCC_FLAG_DERIVE_REVERSE): edge sources,
-    // sorted targets and the sort's temporary storage
-    uint32_t *tsrc = nullptr, *tkey = nullptr;
-    void *ttmp = nullptr;
-    sccb::Ctl *tctl = nullptr;          // error word of scc_derive_reverse
+    // reverse CSR built on the device (SCC_FLAG_DERIVE_REVERSE) and GTgraph
+    // text parsed on the device: the radix sorts' storage
+    uint32_t *tarc[3] = {nullptr, nullptr, nullptr};   // arc-sized sort buffers
+    void *ttmp = nullptr;               // digit histograms and scan sums
+    sccb::Ctl *tctl = nullptr;          // error word of scc_derive_reverse / scc_load_graph_device
     size_t tcapE = 0, ttmp_bytes = 0;
+    char *dtext = nullptr;              // GTgraph text parsed on the device
+    size_t text_cap = 0;
 
     // tuning
     uint32_t tail_vertices = 1024;       // CTA 0 finishes alone at or below this live count
@@ -60,10 +67,15 @@ struct scc_context {
 };
 
 int scc_ctx_reserve(scc_context *ctx, uint32_t V, uint32_t E);
-// Builds Br and Bc (device) from Fr and Fc (device) on stream st; errors in
-// the input are raised in ctx->work.ctl.  Allocates its temporaries in ctx.
+// Builds Br and Bc (device) from Fr (device) and Fc on stream st; errors in
+// the input are raised in ctl.  Allocates its temporaries in ctx.  With hFc
+// set, Fc is still in host memory and is copied to dFc here, in pieces that
+// overlap the first kernels of the build.
 int sccb_derive_reverse(scc_context *ctx, const uint32_t *dFr, const uint32_t *dFc, uint32_t V, uint32_t E,
-                        uint32_t *dBr, uint32_t *dBc, sccb::Ctl *ctl, cudaStream_t st);
+                        uint32_t *dBr, uint32_t *dBc, sccb::Ctl *ctl, cudaStream_t st, const uint32_t *hFc);
+// Device CSR arrays of the context (grown on demand): host inputs are copied
+// there, scc_load_graph_device builds graphs there.
+int sccb_csr_mirror(scc_context *ctx, uint32_t V, uint32_t E);
 // Bytes of the workspace scc_ctx_reserve allocates for a graph.
 size_t scc_ctx_ws_need(uint32_t V, uint32_t E);
 // Raises kernel fn's dynamic shared memory limit on the current device to

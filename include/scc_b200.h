@@ -256,6 +256,18 @@ typedef struct {
 int scc_load_graph(const char *path, scc_host_graph *out);
 /* Write the binary CSR format. */
 int scc_save_binary(const char *path, const scc_host_graph *g);
+/* Write GTgraph text that loadFullGraph reads back as g: seven comment
+ * lines, "p sp V E", then one "a u v 1" line per arc in forward order. */
+int scc_save_gtgraph(const char *path, const scc_host_graph *g);
+/* Read a GTgraph text file (or the binary CSR format) and build both CSRs
+ * on the device (load.cpp:12-113 semantics): the host reads the bytes and
+ * the header, the device parses the arc lines -- one arc "a u v w" per line,
+ * as GTgraph writes them; a line that does not parse, fewer arcs than the
+ * header announces, or an id outside [1, V] gives SCC_ERR_BAD_GRAPH --
+ * orders the arcs by (u, v) and builds the reverse CSR.  *out receives
+ * device pointers into the context's CSR arrays, valid until the next call
+ * of this function or of scc_run with host inputs on the same context. */
+int scc_load_graph_device(scc_context *ctx, const char *path, scc_csr_view *out, void *stream);
 /* Build forward + reverse CSR from E arcs (1-based ids in [1, V]). */
 int scc_graph_from_arcs(uint32_t V, uint64_t E, const uint32_t *src, const uint32_t *dst,
                         scc_host_graph *out);

@@ -85,6 +85,21 @@ def test_cfg2_vslota_rmat22(engine, oracle_lib, permute):
     assert [res.num_trim1, res.num_trim2, res.num_pivot] == [t1, 0, n - t1]
 
 
+def test_cfg2_reverse_csr_built_on_the_device(engine):
+    """The device-built reverse CSR of the R-MAT scale-22 graph equals the
+    reference loader's layout (in-lists in ascending source order)."""
+    import torch
+
+    from detectingscc_b200 import graphs
+    V, Fr, Fc, Br, Bc = _device_graph(lambda dev: graphs.rmat(22, seed=1, device=dev))
+    E = int(Fc.shape[0])
+    dBr = torch.full_like(Br, -1)
+    dBc = torch.full_like(Bc, -1)
+    engine.derive_reverse(V, E, Fr, Fc, dBr, dBc)
+    torch.cuda.synchronize()
+    assert torch.equal(dBr, Br) and torch.equal(dBc, Bc)
+
+
 def test_cfg3_wslota_grid4096(engine, oracle_lib):
     from detectingscc_b200 import graphs
     V, Fr, Fc, Br, Bc = _device_graph(lambda dev: graphs.grid(4096, seed=1, device=dev))

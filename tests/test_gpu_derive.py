@@ -29,6 +29,11 @@ def _cases(golden):
     out.append(("random_dups_loops", 500, rng.integers(1, 501, 6000), rng.integers(1, 501, 6000)))
     V, s, d = graphs.rmat(12, seed=5, clean=False)          # hubs with long in-lists, self-loops, duplicates
     out.append(("rmat12_raw", V, s.numpy(), d.numpy()))
+    # in-lists longer than one shared-memory chunk (4,096): sorted chunks, then merge passes
+    for n in (4097, 9000, 20000):
+        src = rng.permutation(np.arange(2, n + 2))
+        src = np.concatenate([src, src[:100]])              # duplicate arcs into the hub
+        out.append((f"hub_in_{n}", n + 1, src, np.ones(src.size, np.int64)))
     return out
 
 
@@ -88,3 +93,20 @@ def test_bad_forward_csr_is_rejected(engine):
     assert ei.value.code == 23
     # the context still works afterwards
     assert engine.run(g, algo="h", derive_reverse=True).num_sccs == 2
+
+
+def test_host_upload_in_pieces(engine, oracle_lib):
+    """R-MAT scale 20 (raw: hubs, duplicates, self-loops) from host memory with
+    the reverse CSR built on the device: the forward targets cross in eight
+    pieces beside the first kernels of the build; labels equal Tarjan's and
+    the run that copies both CSRs."""
+    from detectingscc_b200 import graphs
+    V, s, d = graphs.rmat(20, seed=9, clean=False)
+    g = scc.graph_from_arcs(V, s.numpy(), d.numpy())
+    assert (g.E + 4095) // 4096 >= 8 * 512                       # 4,096-arc tiles for eight 512-tile pieces
+    for algo in ("h", "g"):
+        a = engine.run(g, algo=algo, derive_reverse=True)
+        b = engine.run(g, algo=algo)
+        lab, n = oracle_lib.tarjan(V, g.Fr, g.Fc)
+        assert np.array_equal(a.labels, lab[1:]) and a.num_sccs == n, algo
+        assert np.array_equal(a.labels, b.labels), algo

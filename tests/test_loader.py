@@ -71,3 +71,19 @@ def test_missing_file(native, tmp_path):
     with pytest.raises(scc.SCCError) as e:
         scc.load_graph(str(tmp_path / "nope.gr"))
     assert "SCC_ERR_IO" in str(e.value)
+
+
+def test_save_gtgraph_roundtrip(native, tmp_path):
+    """The library's GTgraph writer produces what the reference loader
+    (restated) and the product loader read back as the same graph."""
+    rng = np.random.default_rng(4)
+    V = 1000
+    s, d = rng.integers(1, V + 1, 7000), rng.integers(1, V + 1, 7000)
+    g = scc.graph_from_arcs(V, s, d)
+    p = str(tmp_path / "w.gr")
+    scc.save_gtgraph(p, g)
+    V2, E2, Fr, Fc, Br, Bc = load_gtgraph(p)
+    h = scc.load_graph(p)
+    assert (V2, E2) == (g.V, g.E) == (h.V, h.E)
+    for k, ref in zip(("Fr", "Fc", "Br", "Bc"), (Fr, Fc, Br, Bc)):
+        assert np.array_equal(getattr(g, k), ref) and np.array_equal(getattr(h, k), ref), k
