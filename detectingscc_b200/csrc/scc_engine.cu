@@ -354,6 +354,10 @@ extern "C" int scc_destroy(scc_context *ctx)
     if (ctx->htrace) cudaFreeHost(ctx->htrace);
     for (int i = 0; i < 4; i++) if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
     for (auto e : ctx->upev) if (e) cudaEventDestroy(e);
+    for (int i = 0; i < 2; i++) {
+        if (ctx->stage_ev[i]) cudaEventDestroy(ctx->stage_ev[i]);
+        if (ctx->hstage[i]) cudaFreeHost(ctx->hstage[i]);
+    }
     if (ctx->up) cudaStreamDestroy(ctx->up);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;

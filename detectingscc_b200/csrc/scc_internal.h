@@ -38,6 +38,8 @@ struct scc_context {
     size_t tcapE = 0, ttmp_bytes = 0;
     char *dtext = nullptr;              // GTgraph text parsed on the device
     size_t text_cap = 0;
+    char *hstage[2] = {nullptr, nullptr};            // page-locked file staging (scc_load_graph_device)
+    cudaEvent_t stage_ev[2] = {nullptr, nullptr};
 
     // tuning
     uint32_t tail_vertices = 1024;       // CTA 0 finishes alone at or below this live count

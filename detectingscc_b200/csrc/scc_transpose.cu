@@ -715,37 +715,76 @@ extern "C" int scc_derive_reverse(scc_context *ctx, const uint32_t *Fr, const ui
 
 // GTgraph text (or the binary CSR format) -> both CSRs in the context's
 // device arrays; see include/scc_b200.h.
+namespace {
+
+constexpr size_t STAGE = 64u << 20;     // bytes of one page-locked staging buffer
+constexpr size_t HEAD = 1u << 20;       // the text header must end within this many bytes
+
+struct File {
+    FILE *f = nullptr;
+    ~File() { if (f) fclose(f); }
+};
+
+int stage_buffers(scc_context *ctx)
+{
+    for (int i = 0; i < 2; i++) {
+        if (!ctx->hstage[i] && cudaHostAlloc((void **)&ctx->hstage[i], STAGE, cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            return SCC_ERR_OOM;
+        }
+        if (!ctx->stage_ev[i] && cudaEventCreateWithFlags(&ctx->stage_ev[i], cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            return SCC_ERR_CUDA;
+        }
+    }
+    return SCC_OK;
+}
+
+// Bytes [off, off + len) of the file to dst (device) through the two
+// page-locked staging buffers: reading a piece overlaps the copy of the one
+// before.  k counts pieces across calls (which buffer is next).
+int stream_file(scc_context *ctx, FILE *f, uint64_t off, uint64_t len, char *dst, cudaStream_t st, unsigned &k)
+{
+    if (len && fseeko(f, (off_t)off, SEEK_SET) != 0) return SCC_ERR_IO;
+    for (uint64_t done = 0; done < len;) {
+        const size_t n = (size_t)std::min<uint64_t>(STAGE, len - done);
+        const unsigned i = k++ & 1u;
+        if (cudaEventSynchronize(ctx->stage_ev[i]) != cudaSuccess) { cudaGetLastError(); return SCC_ERR_CUDA; }
+        if (fread(ctx->hstage[i], 1, n, f) != n) return SCC_ERR_IO;
+        if (cudaMemcpyAsync(dst + done, ctx->hstage[i], n, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+            cudaEventRecord(ctx->stage_ev[i], st) != cudaSuccess) {
+            cudaGetLastError();
+            return SCC_ERR_CUDA;
+        }
+        done += n;
+    }
+    return SCC_OK;
+}
+
+}  // namespace
+
+// GTgraph text (or the binary CSR format) -> both CSRs in the context's
+// device arrays; see include/scc_b200.h.
 extern "C" int scc_load_graph_device(scc_context *ctx, const char *path, scc_csr_view *out, void *stream)
 {
     if (!ctx || !path || !out) return SCC_ERR_INVALID_ARG;
     memset(out, 0, sizeof(*out));
-    FILE *f = fopen(path, "rb");
-    if (!f) return SCC_ERR_IO;
-    std::vector<char> buf;
-    if (fseek(f, 0, SEEK_END) == 0) {
-        const long sz = ftell(f);
-        if (sz > 0) {
-            try {
-                buf.resize((size_t)sz);
-            } catch (...) {
-                fclose(f);
-                return SCC_ERR_OOM;
-            }
-            fseek(f, 0, SEEK_SET);
-            if (fread(buf.data(), 1, buf.size(), f) != buf.size()) buf.clear();
-        }
-    }
-    fclose(f);
-    if (buf.empty()) return SCC_ERR_IO;
-    const char *s = buf.data(), *e = s + buf.size();
-    uint64_t V = 0, E = 0;
-    const bool bin = buf.size() >= 24 && memcmp(s, "SCCBIN01", 8) == 0;
-    const char *body = nullptr;
+    File file;
+    file.f = fopen(path, "rb");
+    if (!file.f || fseeko(file.f, 0, SEEK_END) != 0) return SCC_ERR_IO;
+    const off_t fsize = ftello(file.f);
+    if (fsize <= 0 || fseeko(file.f, 0, SEEK_SET) != 0) return SCC_ERR_IO;
+    const uint64_t size = (uint64_t)fsize;
+    std::vector<char> hb((size_t)std::min<uint64_t>(size, HEAD));
+    if (fread(hb.data(), 1, hb.size(), file.f) != hb.size()) return SCC_ERR_IO;
+    const char *s = hb.data(), *e = s + hb.size();
+    uint64_t V = 0, E = 0, body_off = 0;
+    const bool bin = size >= 24 && memcmp(s, "SCCBIN01", 8) == 0;
     if (bin) {
         memcpy(&V, s + 8, 8);
         memcpy(&E, s + 16, 8);
         if (V > SCC_MAX_VERTICES || E > SCC_MAX_EDGES) return SCC_ERR_TOO_LARGE;
-        if (buf.size() != 24 + 4 * (2 * (V + 2) + 2 * E)) return SCC_ERR_BAD_GRAPH;
+        if (size != 24 + 4 * (2 * (V + 2) + 2 * E)) return SCC_ERR_BAD_GRAPH;
     } else {
         // load.cpp:32-36: seven header lines, then "p sp V E"
         for (int i = 0; i < 7; i++) {
@@ -759,13 +798,13 @@ extern "C" int scc_load_graph_device(scc_context *ctx, const char *path, scc_csr
             if (q >= e || *q < '0' || *q > '9') return false;
             x = 0;
             while (q < e && *q >= '0' && *q <= '9') x = x * 10 + (uint64_t)(*q++ - '0');
-            return true;
+            return q < e || hb.size() == size;   // a number cut by the end of the header window is not read
         };
         s = tok(ws(s));
         s = tok(ws(s));
         if (!num(s, V) || !num(s, E)) return SCC_ERR_BAD_GRAPH;
         if (V > SCC_MAX_VERTICES || E > SCC_MAX_EDGES) return SCC_ERR_TOO_LARGE;
-        body = s;
+        body_off = (uint64_t)(s - hb.data());
     }
     std::lock_guard<std::mutex> lock(ctx->mu);
     if (cudaSetDevice(ctx->device) != cudaSuccess) { cudaGetLastError(); return SCC_ERR_NO_DEVICE; }
@@ -775,18 +814,23 @@ extern "C" int scc_load_graph_device(scc_context *ctx, const char *path, scc_csr
     if (!ctx->tctl && cudaMalloc((void **)&ctx->tctl, sizeof(Ctl)) != cudaSuccess) { cudaGetLastError(); return SCC_ERR_OOM; }
     if (cudaMemsetAsync(ctx->tctl, 0, sizeof(Ctl), st) != cudaSuccess) { cudaGetLastError(); return SCC_ERR_CUDA; }
     const size_t nv = (size_t)(V + 2) * 4, ne = (size_t)E * 4;
+    if ((rc = stage_buffers(ctx)) != SCC_OK) return rc;
+    unsigned piece = 0;
     if (bin) {
-        const char *p = buf.data() + 24;
-        if (cudaMemcpyAsync(ctx->dFr, p, nv, cudaMemcpyHostToDevice, st) != cudaSuccess ||
-            (E && cudaMemcpyAsync(ctx->dFc, p + nv, ne, cudaMemcpyHostToDevice, st) != cudaSuccess) ||
-            cudaMemcpyAsync(ctx->dBr, p + nv + ne, nv, cudaMemcpyHostToDevice, st) != cudaSuccess ||
-            (E && cudaMemcpyAsync(ctx->dBc, p + 2 * nv + ne, ne, cudaMemcpyHostToDevice, st) != cudaSuccess) ||
-            cudaStreamSynchronize(st) != cudaSuccess) {
+        if ((rc = stream_file(ctx, file.f, 24, nv, (char *)ctx->dFr, st, piece)) != SCC_OK ||
+            (rc = stream_file(ctx, file.f, 24 + nv, ne, (char *)ctx->dFc, st, piece)) != SCC_OK ||
+            (rc = stream_file(ctx, file.f, 24 + nv + ne, nv, (char *)ctx->dBr, st, piece)) != SCC_OK ||
+            (rc = stream_file(ctx, file.f, 24 + 2 * nv + ne, ne, (char *)ctx->dBc, st, piece)) != SCC_OK) {
+            cudaStreamSynchronize(st);
+            cudaGetLastError();
+            return rc;
+        }
+        if (cudaStreamSynchronize(st) != cudaSuccess) {
             cudaGetLastError();
             return SCC_ERR_CUDA;
         }
     } else {
-        const uint64_t L = (uint64_t)(e - body);
+        const uint64_t L = size - body_off;
         const uint64_t nblocks = std::max<uint64_t>((L + (uint64_t)PT * SEG - 1) / ((uint64_t)PT * SEG), 1);
         if (nblocks > 0x7FFFFFFFull) return SCC_ERR_TOO_LARGE;
         if (L + 16 > ctx->text_cap) {
@@ -801,9 +845,10 @@ extern "C" int scc_load_graph_device(scc_context *ctx, const char *path, scc_csr
         if (rc != SCC_OK) return rc;
         uint32_t *src = ctx->dBc, *dst = b.t[2];   // arcs in file order
         uint32_t total = 0;
-        if ((L && cudaMemcpyAsync(ctx->dtext, body, L, cudaMemcpyHostToDevice, st) != cudaSuccess)) {
+        if ((rc = stream_file(ctx, file.f, body_off, L, ctx->dtext, st, piece)) != SCC_OK) {
+            cudaStreamSynchronize(st);
             cudaGetLastError();
-            return SCC_ERR_CUDA;
+            return rc;
         }
         k_parse_count<<<(unsigned)nblocks, PT, 0, st>>>(ctx->dtext, L, (uint32_t)V, b.sums);
         k_scan_sums<<<1, 1024, 0, st>>>(b.sums, (uint32_t)nblocks);
