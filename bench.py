@@ -1,7 +1,7 @@
 """Benchmark of the SCC hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config cfg2|cfg1|cfg3] [--scale S]
+                    [--config cfg1|cfg2|cfg3|cfg4|cfg5] [--scale S] [--permute]
 
 Default workload (the configuration the headline metric is quoted on):
 vSlota with trim-1 and trim-2 flags (-a h -p 1 -q 1) on a seeded synthetic
@@ -71,12 +71,12 @@ CONFIGS = {
 }
 
 
-def _gen_graph(cfg: str, scale: int | None, device):
+def _gen_graph(cfg: str, scale: int | None, device, permute: bool = False):
     from detectingscc_b200 import graphs
     if cfg == "cfg1":
         return graphs.planted_random(seed=1, device=device)
     if cfg == "cfg2":
-        return graphs.rmat(scale or 22, seed=1, device=device)
+        return graphs.rmat(scale or 22, seed=1, device=device, permute=permute)
     if cfg == "cfg3":
         return graphs.grid(scale or 4096, seed=1, device=device)
     raise ValueError(cfg)
@@ -151,10 +151,11 @@ def _host_cpu():
     return {"cpu_model": model, "nproc": os.cpu_count(), "usable_threads": usable}
 
 
-def _config_dict(cfg_name: str, scale, V: int, E: int, world: int) -> dict:
+def _config_dict(cfg_name: str, scale, V: int, E: int, world: int, permute: bool = False) -> dict:
     """The workload description both arms print (same keys and values)."""
     cfg = CONFIGS[cfg_name]
-    return {"workload": f"{cfg_name}: {cfg['desc']}" + (f" [scale override {scale}]" if scale else ""),
+    return {"workload": f"{cfg_name}: {cfg['desc']}" + (f" [scale override {scale}]" if scale else "")
+            + (", vertex ids randomly permuted (seeded, as Graph500 does)" if permute else ""),
             "V": V, "E": E, "seed": 1, "algo": cfg["algo"], "t1": cfg["t1"], "t2": cfg["t2"],
             "warp": cfg["warp"], "l2": "flushed before every step (256 MiB write)",
             "parallelism": "replicas" if world > 1 else "single GPU"}
@@ -220,7 +221,7 @@ def run_ours(args):
     dev = torch.device("cuda", local)
     cfg = CONFIGS[args.config]
 
-    V, s, d = _gen_graph(args.config, args.scale, dev)
+    V, s, d = _gen_graph(args.config, args.scale, dev, args.permute)
     Fr, Fc, Br, Bc = graphs.csr_from_arcs_torch(V, s, d)
     del s, d
     E = int(Fc.shape[0])
@@ -310,7 +311,7 @@ def run_ours(args):
         "vs_baseline": None,
         "dtype": "u32",
         "data": "synthetic (seeded generator, no dataset)",
-        "config": _config_dict(args.config, args.scale, V, E, world),
+        "config": _config_dict(args.config, args.scale, V, E, world, args.permute),
         "num_sccs": int(res.num_sccs),
         "counts": {"trim1": int(res.num_trim1), "trim2": int(res.num_trim2), "pivot": int(res.num_pivot)},
         "passes": res.stats["passes"], "outer_iters": res.stats["outer_iters"],
@@ -419,6 +420,18 @@ def _batch_graphs(n_graphs: int, seed: int = 1, indices=None):
         return list(ex.map(lambda i: scc.graph_from_arcs(*graphs.batch_mix_graph(i, seed=seed)), idx))
 
 
+def cfg4_plan(n_graphs: int, world: int):
+    """cfg4 on `world` ranks: world x n_graphs graphs of the mix (seed 1),
+    split over the ranks by CSR bytes (greedy longest-processing-time; every
+    rank computes the same plan from the sizes alone).  Returns (total
+    graphs, plan) with plan[r] the global indices rank r builds and runs."""
+    from detectingscc_b200 import graphs
+    from detectingscc_b200.shard import shard_by_bytes
+    n_total = n_graphs * world
+    sizes = [graphs.batch_mix_bytes(V, deg) for V, deg in graphs.batch_mix_sizes(n_total, seed=1)]
+    return n_total, shard_by_bytes(sizes, world)
+
+
 def run_batch(args):
     """cfg4: graphs/s of the batched launch vs per-graph plain launches."""
     import torch
@@ -427,13 +440,9 @@ def run_batch(args):
     world, rank, local = _dist_init()
     torch.cuda.set_device(local)
     cfg = CONFIGS["cfg4"]
-    from detectingscc_b200 import graphs
-    from detectingscc_b200.shard import gather_in_order, shard_by_bytes
+    from detectingscc_b200.shard import gather_in_order
     # world x 4096 graphs, sharded by bytes (greedy LPT); each rank builds and runs its own shard
-    n_graphs = args.scale or 4096
-    n_total = n_graphs * world
-    sizes = [graphs.batch_mix_bytes(V, deg) for V, deg in graphs.batch_mix_sizes(n_total, seed=1)]
-    plan = shard_by_bytes(sizes, world)
+    n_total, plan = cfg4_plan(args.scale or 4096, world)
     gs = _batch_graphs(n_total, seed=1, indices=plan[rank])
     eng = scc.Engine(local)
     b = scc.Batch(eng, gs)
@@ -672,7 +681,7 @@ def run_reference(args):
               flush=True)
         return
     dev = torch.device("cuda", local) if torch.cuda.is_available() else torch.device("cpu")
-    V, s, d = _gen_graph(args.config, args.scale, dev)
+    V, s, d = _gen_graph(args.config, args.scale, dev, args.permute)
     Fr, Fc, Br, Bc = (t.cpu().numpy().view(np.uint32) for t in graphs.csr_from_arcs_torch(V, s, d))
     E = int(Fc.shape[0])
     for _ in range(args.warmup):
@@ -690,7 +699,7 @@ def run_reference(args):
         "value": v, "unit": "Medges/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(t * 1e3, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u32", "data": "synthetic (seeded generator, no dataset)",
-        "config": _config_dict(args.config, args.scale, V, E, world),
+        "config": _config_dict(args.config, args.scale, V, E, world, args.permute),
         "cpu_baseline": {"value": v, "unit": "Medges/s", "cores": 1, "kind": "port",
                          "sample": "full graph per step; the reference has no CPU SCC path, so this is the "
                                    "project's iterative Tarjan oracle on one host core", "host": _host_cpu()},
@@ -762,6 +771,7 @@ def main():
     ap.add_argument("--scale", type=int, default=None, help="smaller graph (profiling aid, not a bench value)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-parity", action="store_true", help="skip the label check against the oracle")
+    ap.add_argument("--permute", action="store_true", help="cfg2 with its vertex ids randomly permuted")
     ap.add_argument("--no-file-leg", action="store_true", help="skip the GTgraph file-to-labels measurement")
     args = ap.parse_args()
     world = os.environ.get("WORLD_SIZE")

@@ -102,3 +102,70 @@ def test_two_gloo_ranks_reassemble_the_single_rank_answer(tmp_path):
         assert np.array_equal(np.load(tmp_path / f"counts{r}.npy"), want_counts)
         assert np.array_equal(np.load(tmp_path / f"labels{r}.npy"), want_labels)
     assert np.array_equal(np.load(tmp_path / "counts_dst.npy"), want_counts)
+
+
+def _bench_rank_main(rank, world, port, n, outdir, device):
+    """One rank of bench.py's cfg4 sharding: its plan, its shard built and
+    solved (the batched engine on a GPU, else the oracle), the per-graph
+    results gathered on rank 0 in global order."""
+    import datetime
+
+    import torch.distributed as dist
+
+    import bench
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        n_total, plan = bench.cfg4_plan(n, world)
+        gs = bench._batch_graphs(n_total, seed=1, indices=plan[rank])
+        if device:
+            import detectingscc_b200 as scc
+            eng = scc.Engine(0)
+            b = scc.Batch(eng, gs)
+            try:
+                labels, res, _ = b.run(algo="g", t1=True, t2=True)
+                counts = [int(r[0]) for r in res]
+                labs = [b.labels_of(labels, k).copy() for k in range(len(gs))]
+            finally:
+                b.close()
+                eng.close()
+        else:
+            sol = _solve(gs)
+            counts, labs = [c for c, _ in sol], [lab for _, lab in sol]
+        got_c = gather_in_order(counts, plan, rank, dst=0)
+        got_l = gather_in_order(labs, plan, rank, dst=0)
+        if rank == 0:
+            np.save(os.path.join(outdir, "counts.npy"), np.array(got_c))
+            np.save(os.path.join(outdir, "labels.npy"), np.concatenate(got_l))
+    finally:
+        dist.destroy_process_group()
+
+
+def _bench_cfg4_two_ranks(tmp_path, device):
+    import torch.multiprocessing as mp
+
+    import bench
+    from oracle import oracle
+    oracle.build()
+    n = 12                                       # graphs per rank (the 24 first graphs of the mix)
+    mp.start_processes(_bench_rank_main, args=(2, _free_port(), n, str(tmp_path), device), nprocs=2, join=True,
+                       start_method="spawn")
+    n_total, plan = bench.cfg4_plan(n, 2)
+    assert sorted(plan[0] + plan[1]) == list(range(n_total)) and plan[0] and plan[1]
+    single = _solve(bench._batch_graphs(n_total, seed=1))
+    assert np.array_equal(np.load(tmp_path / "counts.npy"), np.array([c for c, _ in single]))
+    assert np.array_equal(np.load(tmp_path / "labels.npy"), np.concatenate([lab for _, lab in single]))
+
+
+def test_bench_cfg4_sharding_on_two_gloo_ranks(tmp_path):
+    """bench.py --gpus 2 --config cfg4, host side: plan, per-rank shards,
+    gather in global order; the oracle stands in for the device."""
+    _bench_cfg4_two_ranks(tmp_path, device=False)
+
+
+@pytest.mark.gpu
+def test_bench_cfg4_sharding_two_ranks_batched_engine(tmp_path):
+    """The same with each rank's shard run by the batched engine (both ranks
+    on device 0, independent launches): labels equal Tarjan's in order."""
+    _bench_cfg4_two_ranks(tmp_path, device=True)
