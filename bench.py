@@ -323,7 +323,8 @@ def run_ours(args):
                      "T_e_over_E": round(ins["edges_scanned"] / max(E, 1), 3),
                      "T_v_over_V": round(ins["vertex_visits"] / max(V, 1), 3),
                      "B_floor_GBps": round((8 * E + 12 * V) / (t_kern * 1e-3) / 1e9, 1),
-                     "kernel": "k_scc_grid (persistent cooperative SCC kernel)"},
+                     "kernel": "k_scc_block (the whole driver on one CTA)" if res.stats.get("used_block_path")
+                     else "k_scc_grid (persistent cooperative SCC kernel)"},
         "e2e": {"value": round(world * E / (t_e2e * 1e-3) / 1e6, 2), "unit": "Medges/s",
                 "ms_per_step": round(t_e2e, 3),
                 "h2d_bytes_per_step": int(4 * ((V + 2) + E)),

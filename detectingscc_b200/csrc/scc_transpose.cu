@@ -446,52 +446,81 @@ __global__ void k_tr_offsets(const uint32_t *__restrict__ K, uint32_t n, uint32_
 // ---------------------------------------------------------------------
 // GTgraph text parsed on the device (load.cpp:32-77).  The host reads the
 // file and its header (7 lines, then "p sp V E"); the rest -- one arc
-// "a u v w" per line -- is copied to the device and every thread parses
-// the lines that start in its 64-byte segment: one pass counts the arc
-// lines of every segment, a scan gives each segment its first record
-// index, the second pass writes record r's (u, v).  The forward CSR is
-// then two stable radix sorts (by v, then by u) order the arcs by (u, v) as
-// the reference's std::sort does (load.cpp:47), duplicates and self-loops
-// kept, and the reverse CSR is derived from the forward one.
+// "a u v w" per line -- is copied to the device and every thread takes
+// the lines that start in its 64-byte segment, the lanes of a warp one
+// line each per step (so their parses run side by side): one pass counts
+// the records (non-blank lines) of every segment, a scan gives each
+// segment its first record index, the second pass parses and writes record
+// r's (u, v).  Two stable radix sorts (by v, then by u) then order the arcs
+// by (u, v) as the reference's std::sort does (load.cpp:47), duplicates and
+// self-loops kept, and the reverse CSR is derived from the forward one.
 // ---------------------------------------------------------------------
 constexpr uint32_t SEG = 64;            // bytes of text per thread
 constexpr uint32_t PT = 256;            // threads per parse CTA
 
 __device__ __forceinline__ bool tws(char c) { return c == ' ' || c == '\t' || c == '\r'; }
 
-// Parses the line starting at p: 0 blank, 1 an arc (u, v), -1 malformed.
-__device__ int parse_arc(const char *T, uint64_t p, uint64_t L, uint32_t V, uint32_t &u, uint32_t &v)
+// The first line that starts in [b, e) (a line starts at 0 and after every
+// '\n'), or e.
+__device__ __forceinline__ uint64_t first_line(const char *T, uint64_t b, uint64_t e)
 {
-    while (p < L && tws(T[p])) p++;
-    if (p >= L || T[p] == '\n') return 0;
-    p++;   // the arc letter (one character, as the reference reads it, load.cpp:43)
-    uint64_t x[3];
-    for (int k = 0; k < 3; k++) {
-        while (p < L && tws(T[p])) p++;
-        if (p >= L || T[p] < '0' || T[p] > '9') return -1;
-        uint64_t y = 0;
-        while (p < L && T[p] >= '0' && T[p] <= '9') {
-            y = y * 10u + (uint64_t)(T[p] - '0');
-            if (y > 0xFFFFFFFFull) return -1;
-            p++;
-        }
-        x[k] = y;
-    }
-    while (p < L && tws(T[p])) p++;
-    if (p < L && T[p] != '\n') return -1;
-    if (x[0] < 1u || x[0] > V || x[1] < 1u || x[1] > V) return -1;
-    u = (uint32_t)x[0];
-    v = (uint32_t)x[1];
-    return 1;
+    if (b == 0) return 0;
+    uint64_t p = b;
+    while (p < e && T[p - 1] != '\n') p++;
+    return p;
 }
 
-// Arc lines that start in thread t's segment (every thread of the grid).
-__device__ uint32_t seg_arcs(const char *T, uint64_t L, uint32_t V, uint64_t t)
+// Past the '\n' that ends the line p is in (or L).
+__device__ __forceinline__ uint64_t line_end(const char *T, uint64_t p, uint64_t L)
+{
+    while (p < L && T[p] != '\n') p++;
+    return p < L ? p + 1 : L;
+}
+
+// Parses the line starting at p and moves p past it: 0 blank, 1 an arc
+// (u, v), -1 malformed.
+__device__ int parse_line(const char *T, uint64_t &p, uint64_t L, uint32_t V, uint32_t &u, uint32_t &v)
+{
+    int kind = 1;
+    while (p < L && tws(T[p])) p++;
+    if (p >= L || T[p] == '\n') {
+        kind = 0;
+    } else {
+        p++;   // the arc letter (one character, as the reference reads it, load.cpp:43)
+        uint64_t x[3] = {0, 0, 0};
+        for (int k = 0; k < 3 && kind > 0; k++) {
+            while (p < L && tws(T[p])) p++;
+            if (p >= L || T[p] < '0' || T[p] > '9') {
+                kind = -1;
+                break;
+            }
+            uint64_t y = 0;
+            while (p < L && T[p] >= '0' && T[p] <= '9' && y <= 0xFFFFFFFFull) y = y * 10u + (uint64_t)(T[p++] - '0');
+            if (y > 0xFFFFFFFFull) kind = -1;
+            x[k] = y;
+        }
+        if (kind > 0) {
+            while (p < L && tws(T[p])) p++;
+            if ((p < L && T[p] != '\n') || x[0] < 1u || x[0] > V || x[1] < 1u || x[1] > V) kind = -1;
+            u = (uint32_t)x[0];
+            v = (uint32_t)x[1];
+        }
+    }
+    p = line_end(T, p, L);
+    return kind;
+}
+
+// Records (non-blank lines) that start in thread t's segment.  Every lane
+// walks its own lines, all lanes of a warp one line per step.
+__device__ uint32_t seg_records(const char *T, uint64_t L, uint64_t t)
 {
     const uint64_t b = t * SEG, e = min(b + SEG, L);
-    uint32_t n = 0, u, v;
-    for (uint64_t p = b; p < e; p++)
-        if ((p == 0 || T[p - 1] == '\n') && parse_arc(T, p, L, V, u, v) != 0) n++;
+    uint32_t n = 0;
+    for (uint64_t p = first_line(T, b, e); p < e;) {
+        while (p < L && tws(T[p])) p++;
+        if (p < L && T[p] != '\n') n++;
+        p = line_end(T, p, L);
+    }
     return n;
 }
 
@@ -517,10 +546,10 @@ __device__ __forceinline__ uint32_t block_excl256(uint32_t x, uint32_t *total)
     return before + incl - x;
 }
 
-__global__ void __launch_bounds__(PT) k_parse_count(const char *T, uint64_t L, uint32_t V, uint32_t *sums)
+__global__ void __launch_bounds__(PT) k_parse_count(const char *T, uint64_t L, uint32_t *sums)
 {
     uint32_t tot;
-    const uint32_t n = seg_arcs(T, L, V, (uint64_t)blockIdx.x * PT + threadIdx.x);
+    const uint32_t n = seg_records(T, L, (uint64_t)blockIdx.x * PT + threadIdx.x);
     block_excl256(n, &tot);
     if (threadIdx.x == 0) sums[blockIdx.x] = tot;
 }
@@ -533,12 +562,11 @@ __global__ void __launch_bounds__(PT) k_parse_write(const char *T, uint64_t L, u
 {
     uint32_t tot;
     const uint64_t t = (uint64_t)blockIdx.x * PT + threadIdx.x;
-    uint32_t r = sums[blockIdx.x] + block_excl256(seg_arcs(T, L, V, t), &tot);
+    uint32_t r = sums[blockIdx.x] + block_excl256(seg_records(T, L, t), &tot);
     const uint64_t b = t * SEG, e = min(b + SEG, L);
-    for (uint64_t p = b; p < e; p++) {
-        if (p != 0 && T[p - 1] != '\n') continue;
+    for (uint64_t p = first_line(T, b, e); p < e;) {
         uint32_t u = 0, v = 0;
-        const int k = parse_arc(T, p, L, V, u, v);
+        const int k = parse_line(T, p, L, V, u, v);
         if (k < 0) {
             if (r < E) set_error(ctl, E_BAD_GRAPH, 74);   // the reference stops reading after E arcs (load.cpp:42)
             r++;
@@ -850,7 +878,7 @@ extern "C" int scc_load_graph_device(scc_context *ctx, const char *path, scc_csr
             cudaGetLastError();
             return rc;
         }
-        k_parse_count<<<(unsigned)nblocks, PT, 0, st>>>(ctx->dtext, L, (uint32_t)V, b.sums);
+        k_parse_count<<<(unsigned)nblocks, PT, 0, st>>>(ctx->dtext, L, b.sums);
         k_scan_sums<<<1, 1024, 0, st>>>(b.sums, (uint32_t)nblocks);
         k_parse_write<<<(unsigned)nblocks, PT, 0, st>>>(ctx->dtext, L, (uint32_t)V, (uint32_t)E, b.sums, src, dst,
                                                        ctx->tctl);
