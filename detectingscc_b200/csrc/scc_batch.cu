@@ -59,6 +59,7 @@ __device__ void batch_one(Ex &ex, const BatchParams &p, uint32_t gi, char *base,
         carve_work(base, bg.V, bg.E, HONG, &s_w);
         s_w.qcap = p.qcap;
         s_w.bu_k = p.bu_k;
+        s_w.pull_lane = PULL_LANE;
     }
     __syncthreads();
     const Work &w = s_w;

@@ -111,7 +111,11 @@ struct Work {
     Ctl *ctl;
     uint32_t qcap;              // entries per CTA staging queue (dynamic shared memory)
     uint32_t bu_k;              // bottom-up BFS step when frontier edges > bu_k * scope vertices (0 = never)
+    uint32_t pull_lane;         // bottom-up step: lists up to this many entries are tested by their lane alone;
+                                // of a longer list the lane tests the first min(8, pull_lane), the warp the rest
 };
+
+constexpr uint32_t PULL_LANE = 32;   // Work::pull_lane of the batched and no-allocation paths
 
 // Carve the work arrays for a graph of V vertices and E edges out of `base`
 // (nullptr: only count).  Returns the bytes used.  Same layout on host and

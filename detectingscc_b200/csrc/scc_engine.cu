@@ -490,6 +490,7 @@ extern "C" int scc_run(scc_context *ctx, const scc_csr_view *gv, int algo, uint3
 
     ctx->work.qcap = ctx->qcap;
     ctx->work.bu_k = ctx->bu_k;
+    ctx->work.pull_lane = ctx->pull_lane;
     const size_t smem_block = dyn_smem_bytes(ctx->qcap, 2), smem_grid = dyn_smem_bytes(ctx->qcap, 3);
     Params p{g, ctx->work, (flags & SCC_FLAG_TRIM1) ? 1 : 0, (flags & SCC_FLAG_TRIM2) ? 1 : 0, lw, ctx->tail_vertices,
              dout, ctx->max_passes, ctx->hold_pass};
@@ -555,6 +556,10 @@ extern "C" int scc_set_tuning(scc_context *ctx, const char *key, long long value
     else if (!strcmp(key, "timeout_ms")) ctx->timeout_ms = (uint32_t)value;
     else if (!strcmp(key, "max_blocks_per_sm")) ctx->max_blocks_per_sm = (int)value;
     else if (!strcmp(key, "bu_k")) ctx->bu_k = (uint32_t)value;
+    else if (!strcmp(key, "pull_lane")) {
+        if (value < 1 || value > 1024) return SCC_ERR_INVALID_ARG;
+        ctx->pull_lane = (uint32_t)value;
+    }
     else if (!strcmp(key, "cluster_check")) ctx->cluster_check = value ? 1 : 0;
     else if (!strcmp(key, "max_passes")) ctx->max_passes = (uint32_t)value;
     else if (!strcmp(key, "test_withhold_arrival")) ctx->hold_pass = (uint32_t)value;

@@ -198,6 +198,7 @@ extern "C" int scc_run_noalloc(const scc_csr_view *gv, int algo, uint32_t flags,
     w.ctl = (Ctl *)take(sizeof(Ctl));
     w.qcap = NOALLOC_QCAP;
     w.bu_k = 2;
+    w.pull_lane = PULL_LANE;
     if (off > NOALLOC_BYTES) return SCC_ERR_TOO_LARGE;
 
     cudaStream_t st = (cudaStream_t)stream;

@@ -527,12 +527,13 @@ __device__ __forceinline__ void bfs_pull2(Ex &ex, const Graph &g, const Work &w,
         want[2 * h + 1] = (s[h] & RMASK) | BVB;
     }
     unsigned scanned = 0;
-    uint32_t lim[4];   // the lane scans a list to its end if it is short, else its first 8 entries
+    uint32_t lim[4];   // the lane scans a list to its end if it is short, else its first entries
+    const uint32_t first = min(8u, w.pull_lane);
 #pragma unroll
     for (int t = 0; t < 4; t++) {
         found[t] = false;
         on[t] = end[t] > pos[t];
-        lim[t] = end[t] - pos[t] <= 32u ? end[t] : pos[t] + 8u;
+        lim[t] = end[t] - pos[t] <= w.pull_lane ? end[t] : pos[t] + first;
     }
     // by the lane: two entries of every open search per step (a visited
     // neighbour is usually among the first entries, the lowest ids)

@@ -132,6 +132,10 @@ int scc_derive_reverse(scc_context *ctx, const uint32_t *Fr, const uint32_t *Fc,
  *   "bu_k"                bottom-up BFS step when the frontier's edges exceed
  *                         bu_k * (vertices the search can reach) (default 2,
  *                         0 = never)
+ *   "pull_lane"           bottom-up step: adjacency lists up to this length
+ *                         are tested by their lane alone; of a longer list
+ *                         the lane tests the first min(8, pull_lane) entries
+ *                         and the whole warp the rest (1..1024, default 4)
  *   "qcap"                entries of each warp's shared-memory staging slice
  *                         (32..576; 3 queues x 32 warps x qcap x 4 bytes on
  *                         the whole-GPU kernel, 2 queues on one CTA)
