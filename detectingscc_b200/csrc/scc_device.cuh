@@ -513,13 +513,21 @@ __device__ __forceinline__ void bq_flush(unsigned nq, uint32_t qcap, uint32_t *g
 {
     __syncthreads();
     const unsigned nw = blockDim.x >> 5;
-    if (threadIdx.x == 0) {
-        for (unsigned qi = 0; qi < nq; qi++) {
-            unsigned total = 0;
-            for (unsigned wi = 0; wi < nw; wi++) {
-                sccb_dsmem[BQ_PRE + qi * BQ_WARPS + wi] = total;
-                total += sccb_dsmem[BQ_CNT + qi * BQ_WARPS + wi];
-            }
+    const unsigned wi = threadIdx.x >> 5;
+    // warp q lays out queue q: the warps' fill counts scanned by shuffles,
+    // one global atomicAdd for the CTA's room; the queues' atomics overlap
+    for (unsigned qi = wi; qi < nq; qi += nw) {
+        const unsigned ln = lane_id();
+        const unsigned c = ln < nw ? sccb_dsmem[BQ_CNT + qi * BQ_WARPS + ln] : 0u;
+        unsigned incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(FULL, incl, o);
+            if (ln >= (unsigned)o) incl += y;
+        }
+        if (ln < nw) sccb_dsmem[BQ_PRE + qi * BQ_WARPS + ln] = incl - c;
+        const unsigned total = __shfl_sync(FULL, incl, 31);
+        if (ln == 0) {
             sccb_dsmem[8 + qi] = total ? atomicAdd(qi == 2 ? gcnt2 : qi ? gcnt1 : gcnt0, total) : 0u;
             unsigned *ec = qi == 2 ? nullptr : qi ? ecnt1 : ecnt0;
             if (ec && sccb_dsmem[12 + qi]) atomicAdd(ec, sccb_dsmem[12 + qi]);
@@ -527,7 +535,6 @@ __device__ __forceinline__ void bq_flush(unsigned nq, uint32_t qcap, uint32_t *g
         }
     }
     __syncthreads();
-    const unsigned wi = threadIdx.x >> 5;
     for (unsigned qi = 0; qi < nq; qi++) {
         uint32_t *gq = qi == 2 ? gq2 : qi ? gq1 : gq0;
         const unsigned cnt = sccb_dsmem[BQ_CNT + qi * BQ_WARPS + wi];
@@ -757,10 +764,9 @@ __device__ __forceinline__ void block_min_atomic(uint32_t x, uint32_t *dst)
     const unsigned wi = threadIdx.x >> 5, nw = blockDim.x >> 5;
     if (lane_id() == 0) s_min[wi] = m;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        uint32_t r = 0xFFFFFFFFu;
-        for (unsigned i = 0; i < nw; i++) r = min(r, s_min[i]);
-        if (r != 0xFFFFFFFFu && r < *(volatile uint32_t *)dst) atomicMin(dst, r);
+    if (wi == 0) {
+        const uint32_t r = __reduce_min_sync(FULL, lane_id() < nw ? s_min[lane_id()] : 0xFFFFFFFFu);
+        if (lane_id() == 0 && r != 0xFFFFFFFFu && r < *(volatile uint32_t *)dst) atomicMin(dst, r);
     }
     __syncthreads();
 }
@@ -777,10 +783,12 @@ __device__ __forceinline__ void block_max_atomic(unsigned long long key, unsigne
     unsigned w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     if (lane_id() == 0) s_red[w] = wk;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        unsigned long long m = 0;
-        for (unsigned i = 0; i < nw; i++) m = s_red[i] > m ? s_red[i] : m;
-        if (m && m > *(volatile unsigned long long *)dst) atomicMax(dst, m);
+    if (w == 0) {
+        const unsigned long long k = lane_id() < nw ? s_red[lane_id()] : 0ull;
+        const unsigned khi = __reduce_max_sync(FULL, (unsigned)(k >> 32));
+        const unsigned klo = __reduce_max_sync(FULL, (unsigned)(k >> 32) == khi ? (unsigned)k : 0u);
+        const unsigned long long m = ((unsigned long long)khi << 32) | klo;
+        if (lane_id() == 0 && m && m > *(volatile unsigned long long *)dst) atomicMax(dst, m);
     }
     __syncthreads();
 }
