@@ -87,7 +87,7 @@ MAX_VERTICES = 268435454
 # every symbol include/scc_b200.h and include/scc_compat.h declare
 C_SYMBOLS = ["scc_create", "scc_destroy", "scc_run", "scc_set_tuning", "scc_status_string",
              "scc_version", "scc_get_trace", "scc_derive_reverse", "scc_load_graph", "scc_save_binary", "scc_graph_from_arcs",
-             "scc_free_host_graph", "scc_save_gtgraph", "scc_load_graph_device", "scc_save_metis", "scc_load_partition", "scc_detect", "scc_reference_detect",
+             "scc_free_host_graph", "scc_run_async", "scc_finish", "scc_save_gtgraph", "scc_load_graph_device", "scc_save_metis", "scc_load_partition", "scc_detect", "scc_reference_detect",
              "scc_reference_call", "scc_batch_create", "scc_batch_run",
              "scc_batch_destroy", "scc_run_noalloc", "scc_batch_set_schedule", "scc_batch_get_schedule",
              "scc_batch_autotune", "scc_batch_info", "scc_batch_set_cluster", "scc_batch_get_cluster", "scc_server_create", "scc_server_submit",
@@ -123,6 +123,8 @@ def lib():
     L.scc_destroy.argtypes = [vp]
     L.scc_run.argtypes = [vp, ctypes.POINTER(CsrView), ctypes.c_int, u32, ctypes.c_int, vp,
                           ctypes.POINTER(Stats), vp]
+    L.scc_run_async.argtypes = [vp, ctypes.POINTER(CsrView), ctypes.c_int, u32, ctypes.c_int, vp, vp]
+    L.scc_finish.argtypes = [vp, ctypes.POINTER(Stats)]
     L.scc_set_tuning.argtypes = [vp, ctypes.c_char_p, ctypes.c_longlong]
     L.scc_status_string.restype = ctypes.c_char_p
     L.scc_status_string.argtypes = [ctypes.c_int]

@@ -181,12 +181,16 @@ class Engine:
                 "scc_derive_reverse")
 
     def run_device(self, V: int, E: int, Fr, Fc, Br, Bc, labels_out=None, algo="h", t1=True, t2=True,
-                   warp=1, instrument=False, stream=None, force=None, derive_reverse: bool = False) -> Result:
+                   warp=1, instrument=False, stream=None, force=None, derive_reverse: bool = False,
+                   wait: bool = True) -> Optional[Result]:
         """Run on device-resident CSR (torch CUDA tensors or raw device pointers).
 
         labels_out: device buffer of V uint32/int32 entries, or None.
         stream: a cudaStream_t handle (int); None means the current PyTorch stream
                 of the tensors' device (or the legacy default stream for raw pointers).
+        wait: False enqueues the run and returns None at once (scc_run_async);
+              labels_out is complete in the stream's order and finish() returns
+              the Result.
         """
         flags = N.FLAG_DEVICE | (N.FLAG_TRIM1 if t1 else 0) | (N.FLAG_TRIM2 if t2 else 0)
         flags |= N.FLAG_INSTRUMENT if instrument else 0
@@ -200,10 +204,21 @@ class Engine:
             import torch
             stream = torch.cuda.current_stream(Fr.device).cuda_stream
         view = N.CsrView(int(V), int(E), _ptr(Fr), _ptr(Fc), _ptr(Br), _ptr(Bc))
+        if not wait:
+            N.check(self._lib.scc_run_async(self._h, ctypes.byref(view), _algo_code(algo), flags, int(warp),
+                                            _ptr(labels_out), stream), "scc_run_async")
+            return None
         st = N.Stats()
         rc = self._lib.scc_run(self._h, ctypes.byref(view), _algo_code(algo), flags, int(warp),
                                _ptr(labels_out), ctypes.byref(st), stream)
         N.check(rc, f"scc_run (device error location {st.error_where})" if rc else "scc_run")
+        return Result(None, st.num_sccs, st.num_trim1, st.num_trim2, st.num_pivot, st.as_dict())
+
+    def finish(self) -> Result:
+        """Waits for the last run_device(..., wait=False) and returns its Result."""
+        st = N.Stats()
+        rc = self._lib.scc_finish(self._h, ctypes.byref(st))
+        N.check(rc, f"scc_finish (device error location {st.error_where})" if rc else "scc_finish")
         return Result(None, st.num_sccs, st.num_trim1, st.num_trim2, st.num_pivot, st.as_dict())
 
 

@@ -68,6 +68,17 @@ struct __align__(128) Ctl {
                                                    // keep the FV|BV mark (lazy Slota update); ~0 before
 };
 
+// A control block reset on the device (k_canon_write), as the host would
+// initialise it: zero, then the fields below; pivkey: one pivot word to
+// clear as well, or nullptr.
+struct CtlReset {
+    Ctl *next;
+    unsigned long long timeout_ns;
+    unsigned long long *trace;
+    unsigned trace_cap;
+    unsigned long long *pivkey;
+};
+
 // Phase ids recorded in the pass trace.
 enum {
     PH_INIT = 1, PH_TRIM1_ONCE = 2, PH_TRIM1_APPLY = 3, PH_TRIM1_FIX = 4, PH_TRIM2 = 5, PH_TRIM2_APPLY = 6,

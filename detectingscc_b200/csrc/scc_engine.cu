@@ -145,8 +145,22 @@ __global__ void __launch_bounds__(BLOCK_THREADS, 1) k_scc_block(Params p)
 // which the update passes fold into smin[representative].
 // Skipped when the SCC kernel already wrote them (ctl->labels_done).
 __global__ void k_canon_write(const uint32_t *__restrict__ label, const uint32_t *__restrict__ smin,
-                              const uint32_t *__restrict__ st, uint32_t *__restrict__ out, uint32_t V, const Ctl *ctl)
+                              const uint32_t *__restrict__ st, uint32_t *__restrict__ out, uint32_t V, const Ctl *ctl,
+                              CtlReset r)
 {
+    if (blockIdx.x == 0 && r.next) {
+        // the next run's control block, as the host would write it
+        unsigned *wd = reinterpret_cast<unsigned *>(r.next);
+        for (unsigned i = threadIdx.x; i < sizeof(Ctl) / 4u; i += blockDim.x) wd[i] = 0u;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            r.next->first_min = 0xFFFFFFFFu;
+            r.next->timeout_ns = r.timeout_ns;
+            r.next->trace = r.trace;
+            r.next->trace_cap = r.trace_cap;
+            if (r.pivkey) *r.pivkey = 0ull;
+        }
+    }
     if (ctl && ctl->labels_done) return;
     canon_labels(label, smin, st, ctl ? ctl->first_min : 0xFFFFFFFFu, out, V, blockIdx.x * blockDim.x + threadIdx.x,
                  gridDim.x * blockDim.x);
@@ -348,7 +362,7 @@ extern "C" int scc_destroy(scc_context *ctx)
     cudaFree(ctx->ws);
     cudaFree(ctx->dFr); cudaFree(ctx->dFc); cudaFree(ctx->dBr); cudaFree(ctx->dBc); cudaFree(ctx->dlab);
     for (auto *p : ctx->tarc) cudaFree(p);
-    cudaFree(ctx->ttmp); cudaFree(ctx->tctl); cudaFree(ctx->dtext);
+    cudaFree(ctx->ttmp); cudaFree(ctx->tctl); cudaFree(ctx->dtext); cudaFree(ctx->ctlb[0]);
     if (ctx->hctl) cudaFreeHost(ctx->hctl);
     cudaFree(ctx->dtrace);
     if (ctx->htrace) cudaFreeHost(ctx->htrace);
@@ -414,11 +428,38 @@ static int prepare_kernel(scc_context *ctx, void *fn, size_t smem, int threads)
     return nb;
 }
 
-extern "C" int scc_run(scc_context *ctx, const scc_csr_view *gv, int algo, uint32_t flags, int warp_width,
-                       uint32_t *labels_out, scc_stats *stats, void *stream_arg)
+// Counters and times of the run that ended with ctx->ev[3] (complete).
+static int read_result(scc_context *ctx, scc_stats *stats)
+{
+    const Ctl &c = *ctx->hctl;
+    if (stats) {
+        stats->num_trim1 = c.n_trim1;
+        stats->num_trim2 = c.n_trim2;
+        stats->num_pivot = c.n_pivot;
+        stats->num_sccs = c.n_trim1 + c.n_trim2 + c.n_pivot;
+        stats->edges_scanned = c.t_edges;
+        stats->vertex_visits = c.t_verts;
+        stats->passes = c.passes;
+        stats->outer_iters = c.outer;
+        stats->tail_pass = c.tail_pass;
+        stats->gpu_launches = ctx->pend_launches;
+        stats->grid_blocks = ctx->pend_blocks;
+        stats->used_block_path = ctx->pend_block_path;
+        cudaEventElapsedTime(&stats->kernel_ms, ctx->ev[1], ctx->ev[2]);
+        cudaEventElapsedTime(&stats->total_ms, ctx->ev[0], ctx->ev[3]);
+        stats->error_where = c.where;
+    }
+    return c.error ? c.error : SCC_OK;
+}
+
+// scc_run and scc_run_async: everything up to the last copy of the run is
+// enqueued on the stream; async returns there, scc_run waits and reads.
+static int run_impl(scc_context *ctx, const scc_csr_view *gv, int algo, uint32_t flags, int warp_width,
+                    uint32_t *labels_out, scc_stats *stats, void *stream_arg, bool async)
 {
     if (!ctx || !gv) return SCC_ERR_INVALID_ARG;
     if (stats) memset(stats, 0, sizeof(*stats));
+    if (async && !(flags & SCC_FLAG_DEVICE)) return SCC_ERR_INVALID_ARG;
     const bool hong = algo == SCC_ALGO_VHONG || algo == SCC_ALGO_WHONG;
     const bool warped = algo == SCC_ALGO_WHONG || algo == SCC_ALGO_WSLOTA;
     if (!hong && algo != SCC_ALGO_VSLOTA && algo != SCC_ALGO_WSLOTA) return SCC_ERR_INVALID_ARG;
@@ -472,20 +513,39 @@ extern "C" int scc_run(scc_context *ctx, const scc_csr_view *gv, int algo, uint3
     if (!E) { g.Fc = g.Fc ? g.Fc : ctx->work.st; g.Bc = g.Bc ? g.Bc : ctx->work.st; }
     g.vec = ((((uintptr_t)g.Fr) | ((uintptr_t)g.Br)) & 15u) == 0u ? 1u : 0u;
 
-    // control block: zeroed, then the timeout
-    memset(ctx->hctl, 0, sizeof(Ctl));
-    ctx->hctl->first_min = 0xFFFFFFFFu;
-    ctx->hctl->timeout_ns = (unsigned long long)ctx->timeout_ms * 1000000ull;
-    ctx->hctl->trace = ctx->dtrace;
-    ctx->hctl->trace_cap = ctx->dtrace ? ctx->trace_cap : 0u;
-    CK(cudaMemcpyAsync(ctx->work.ctl, ctx->hctl, sizeof(Ctl), cudaMemcpyHostToDevice, st));
+    // control block: zeroed, then the timeout.  Two blocks alternate; the
+    // label kernel of a run resets the other one for the next run, which
+    // then needs no copy from the host (same timeout and trace settings).
+    if (!ctx->ctlb[0]) {
+        Ctl *b2 = nullptr;
+        if (cudaMalloc((void **)&b2, 2 * sizeof(Ctl)) != cudaSuccess) { cudaGetLastError(); return SCC_ERR_OOM; }
+        ctx->ctlb[0] = b2;
+        ctx->ctlb[1] = b2 + 1;
+    }
+    const int ci = ctx->ctl_next;
+    ctx->ctl_next = ci ^ 1;
+    const CtlReset init{ctx->ctlb[ci ^ 1], (unsigned long long)ctx->timeout_ms * 1000000ull, ctx->dtrace,
+                        ctx->dtrace ? ctx->trace_cap : 0u, hong ? nullptr : ctx->work.pivkey};
+    const bool ready = ctx->ctl_ready[ci] && ctx->ctl_made[ci].timeout_ns == init.timeout_ns &&
+                       ctx->ctl_made[ci].trace == init.trace && ctx->ctl_made[ci].trace_cap == init.trace_cap;
+    const bool piv_ready = ready && !hong && ctx->ctl_made[ci].pivkey == ctx->work.pivkey;
+    ctx->ctl_ready[ci] = false;
+    ctx->work.ctl = ctx->ctlb[ci];
+    if (!ready) {
+        memset(ctx->hctl, 0, sizeof(Ctl));
+        ctx->hctl->first_min = 0xFFFFFFFFu;
+        ctx->hctl->timeout_ns = init.timeout_ns;
+        ctx->hctl->trace = init.trace;
+        ctx->hctl->trace_cap = init.trace_cap;
+        CK(cudaMemcpyAsync(ctx->work.ctl, ctx->hctl, sizeof(Ctl), cudaMemcpyHostToDevice, st));
+    }
     if (derive) {
         // after the control block is zeroed: input errors found here stop the SCC kernel at its entry
         rc = sccb_derive_reverse(ctx, g.Fr, g.Fc, V, E, const_cast<uint32_t *>(g.Br), const_cast<uint32_t *>(g.Bc),
                                  ctx->work.ctl, st, dev ? nullptr : gv->Fc);
         if (rc != SCC_OK) return rc;
     }
-    CK(cudaMemsetAsync(ctx->work.pivkey, 0, hong ? (4 * ((size_t)V + 1) + 8) * 8 : 8, st));
+    if (!piv_ready) CK(cudaMemsetAsync(ctx->work.pivkey, 0, hong ? (4 * ((size_t)V + 1) + 8) * 8 : 8, st));
 
 
     ctx->work.qcap = ctx->qcap;
@@ -516,35 +576,50 @@ extern "C" int scc_run(scc_context *ctx, const scc_csr_view *gv, int algo, uint3
     CK(cudaEventRecord(ctx->ev[2], st));
     if (dout) {
         k_canon_write<<<canon_ctas(V), 256, 0, st>>>(ctx->work.label, ctx->work.smin, ctx->work.st, dout, V,
-                                                     ctx->work.ctl);
+                                                     ctx->work.ctl, init);
         launches += 1;
         CK(cudaGetLastError());
+        ctx->ctl_made[ci ^ 1] = init;
+        ctx->ctl_ready[ci ^ 1] = true;
         if (!dev) CK(cudaMemcpyAsync(labels_out, dout, (size_t)V * 4, cudaMemcpyDeviceToHost, st));
     }
     CK(cudaMemcpyAsync(ctx->hctl, ctx->work.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
     if (ctx->dtrace) CK(cudaMemcpyAsync(ctx->htrace, ctx->dtrace, (size_t)ctx->trace_cap * 16, cudaMemcpyDeviceToHost, st));
     CK(cudaEventRecord(ctx->ev[3], st));
+    ctx->pend_launches = launches;
+    ctx->pend_blocks = (uint32_t)nblocks;
+    ctx->pend_block_path = use_block ? 1u : 0u;
+    ctx->pending = true;
+    if (async) return SCC_OK;
     CK(cudaStreamSynchronize(st));
-    const Ctl &c = *ctx->hctl;
-    if (stats) {
-        stats->num_trim1 = c.n_trim1;
-        stats->num_trim2 = c.n_trim2;
-        stats->num_pivot = c.n_pivot;
-        stats->num_sccs = c.n_trim1 + c.n_trim2 + c.n_pivot;
-        stats->edges_scanned = c.t_edges;
-        stats->vertex_visits = c.t_verts;
-        stats->passes = c.passes;
-        stats->outer_iters = c.outer;
-        stats->tail_pass = c.tail_pass;
-        stats->gpu_launches = launches;
-        stats->grid_blocks = (uint32_t)nblocks;
-        stats->used_block_path = use_block ? 1u : 0u;
-        cudaEventElapsedTime(&stats->kernel_ms, ctx->ev[1], ctx->ev[2]);
-        cudaEventElapsedTime(&stats->total_ms, ctx->ev[0], ctx->ev[3]);
-        stats->error_where = c.where;
+    ctx->pending = false;
+    return read_result(ctx, stats);
+}
+
+extern "C" int scc_run(scc_context *ctx, const scc_csr_view *gv, int algo, uint32_t flags, int warp_width,
+                       uint32_t *labels_out, scc_stats *stats, void *stream_arg)
+{
+    return run_impl(ctx, gv, algo, flags, warp_width, labels_out, stats, stream_arg, false);
+}
+
+extern "C" int scc_run_async(scc_context *ctx, const scc_csr_view *gv, int algo, uint32_t flags, int warp_width,
+                             uint32_t *labels_out, void *stream)
+{
+    return run_impl(ctx, gv, algo, flags, warp_width, labels_out, nullptr, stream, true);
+}
+
+extern "C" int scc_finish(scc_context *ctx, scc_stats *stats)
+{
+    if (!ctx) return SCC_ERR_INVALID_ARG;
+    if (stats) memset(stats, 0, sizeof(*stats));
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    if (!ctx->pending) return SCC_OK;
+    if (cudaSetDevice(ctx->device) != cudaSuccess || cudaEventSynchronize(ctx->ev[3]) != cudaSuccess) {
+        cudaGetLastError();
+        return SCC_ERR_CUDA;
     }
-    if (c.error) return c.error;
-    return SCC_OK;
+    ctx->pending = false;
+    return read_result(ctx, stats);
 }
 
 extern "C" int scc_set_tuning(scc_context *ctx, const char *key, long long value)
@@ -613,7 +688,7 @@ int sccb_launch_block_path(const Graph &g, const Work &w, int t1, int t2, int lw
     void *args[] = {&p};
     cudaError_t e = cudaLaunchKernel(fn, dim3(1), dim3(BLOCK_THREADS), args, smem, st);
     if (e != cudaSuccess) return cuda_status(e);
-    k_canon_write<<<canon_ctas(g.V), 256, 0, st>>>(w.label, w.smin, w.st, dout, g.V, w.ctl);
+    k_canon_write<<<canon_ctas(g.V), 256, 0, st>>>(w.label, w.smin, w.st, dout, g.V, w.ctl, CtlReset{});
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_status(e);
     *launches = 2;

@@ -36,6 +36,15 @@ struct scc_context {
     void *ttmp = nullptr;               // digit histograms and scan sums
     sccb::Ctl *tctl = nullptr;          // error word of scc_derive_reverse / scc_load_graph_device
     size_t tcapE = 0, ttmp_bytes = 0;
+    // two control blocks used in turn; made[i] records how block i was last
+    // reset by a label kernel (ready[i]: not used since)
+    sccb::Ctl *ctlb[2] = {nullptr, nullptr};
+    int ctl_next = 0;
+    bool ctl_ready[2] = {false, false};
+    sccb::CtlReset ctl_made[2] = {};
+    // the last run's launch facts, read back by scc_finish after scc_run_async
+    bool pending = false;
+    unsigned pend_launches = 0, pend_blocks = 0, pend_block_path = 0;
     char *dtext = nullptr;              // GTgraph text parsed on the device
     size_t text_cap = 0;
     char *hstage[2] = {nullptr, nullptr};            // page-locked file staging (scc_load_graph_device)

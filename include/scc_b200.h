@@ -113,6 +113,18 @@ int scc_destroy(scc_context *ctx);
 int scc_run(scc_context *ctx, const scc_csr_view *g, int algo, uint32_t flags, int warp_width,
             uint32_t *labels_out, scc_stats *stats, void *stream);
 
+/* scc_run without the wait, for device-resident pipelines: the same work is
+ * enqueued on `stream` (SCC_FLAG_DEVICE required: inputs and labels_out are
+ * device pointers) and the call returns; labels_out is complete in the
+ * stream's order.  scc_finish waits for the last run enqueued on the
+ * context and returns its status and stats (the same as scc_run's).  Until
+ * then the context's workspace belongs to that run: the next run on the
+ * context must be on the same stream or after scc_finish.  No counterpart in
+ * the reference, whose drivers block on the host after every BFS level. */
+int scc_run_async(scc_context *ctx, const scc_csr_view *g, int algo, uint32_t flags, int warp_width,
+                  uint32_t *labels_out, void *stream);
+int scc_finish(scc_context *ctx, scc_stats *stats);
+
 /* The reverse CSR built on the device from the forward one, in the reference
  * loader's layout (load.cpp:47-113: Br[0] = Br[1] = 0, in-lists in ascending
  * source order).  All pointers are device pointers; Br has V+2 entries, Bc E.
