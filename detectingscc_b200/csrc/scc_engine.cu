@@ -47,16 +47,22 @@ constexpr uint32_t LABEL_UNROLL = 4;
 // A vertex whose state still carries both visited bits with range 0 is a
 // member of the first pivot's SCC left marked by the lazy Slota update; its
 // label is first_min.
+// SKIP_RESIDUAL: vertices still carrying the residual solver's tag
+// (FV|BV|(i+1)) are left out; the solver writes theirs.
+template <bool SKIP_RESIDUAL = false>
 __device__ __forceinline__ void canon_labels(const uint32_t *label, const uint32_t *smin, const uint32_t *st,
                                              uint32_t first_min, uint32_t *out, uint32_t V, uint32_t tid, uint32_t n)
 {
     for (uint32_t v0 = tid + 1u; v0 <= V; v0 += LABEL_UNROLL * n) {
         uint32_t l[LABEL_UNROLL];
+        bool skip[LABEL_UNROLL];
 #pragma unroll
         for (uint32_t j = 0; j < LABEL_UNROLL; ++j) {
             const uint32_t v = v0 + j * n;
             l[j] = v <= V ? label[v] : 0xFFFFFFFFu;
-            if (v <= V && st[v] == (FVB | BVB)) l[j] = LBL_SELF | first_min;
+            const uint32_t s = v <= V ? st[v] : DEAD;
+            if (s == (FVB | BVB)) l[j] = LBL_SELF | first_min;
+            skip[j] = SKIP_RESIDUAL && (s & (FVB | BVB)) == (FVB | BVB) && (s & RMASK) != 0u;
         }
 #pragma unroll
         for (uint32_t j = 0; j < LABEL_UNROLL; ++j)
@@ -64,7 +70,7 @@ __device__ __forceinline__ void canon_labels(const uint32_t *label, const uint32
 #pragma unroll
         for (uint32_t j = 0; j < LABEL_UNROLL; ++j) {
             const uint32_t v = v0 + j * n;
-            if (v <= V) out[v - 1u] = l[j];
+            if (v <= V && !skip[j]) out[v - 1u] = l[j];
         }
     }
 }
@@ -98,10 +104,24 @@ __global__ void __launch_bounds__(GRID_THREADS, 1) k_scc_grid(Params p)
     if (rc == RUN_DONE) rc = HONG ? hong_loop(ex, p.g, p.w, cy, p.tail_n) : slota_peels(ex, p.g, p.w, cy, p.tail_n);
     if (rc == RUN_RESIDUAL) {
         // the live vertices fit one CTA's shared memory: CTA 0 solves them
-        if (blockIdx.x != 0) return;
-        res_solve(p.g, p.w, p.w.L[cy.lsel], cy.nL, p.w.Q[1][(cy.gl - 1u) & 1u], last_count(ex, C_BQ), p.w.ctl);
+        // while the other CTAs write every other vertex's label (every SCC
+        // outside the residual is final here)
+        if (blockIdx.x != 0) {
+            if (p.out)
+                canon_labels<true>(p.w.label, p.w.smin, p.w.st, *(volatile const uint32_t *)&p.w.ctl->first_min, p.out,
+                                   p.g.V, (blockIdx.x - 1u) * blockDim.x + threadIdx.x, (gridDim.x - 1u) * blockDim.x);
+            return;
+        }
+        res_solve(p.g, p.w, p.w.L[cy.lsel], cy.nL, p.w.Q[1][(cy.gl - 1u) & 1u], last_count(ex, C_BQ), p.w.ctl,
+                  p.out);
         res_trace(p.w.ctl, cy.gl, cy.nL);
-        if (threadIdx.x == 0) { p.w.ctl->tail_pass = cy.gl; p.w.ctl->nlive_tail = cy.nL; p.w.ctl->passes = cy.gl + 1u; }
+        if (threadIdx.x == 0) {
+            p.w.ctl->tail_pass = cy.gl;
+            p.w.ctl->nlive_tail = cy.nL;
+            p.w.ctl->passes = cy.gl + 1u;
+            // the labels are complete when the kernel ends (a failed solve leaves them to k_canon_write)
+            if (p.out && !*(volatile int *)&p.w.ctl->error) p.w.ctl->labels_done = 1u;
+        }
         return;
     }
     if (rc == RUN_SWITCH) {

@@ -1187,8 +1187,11 @@ __device__ bool res_extract(Ex &ex, const Graph &g, const Work &w, Carry &cy)
 // adds the SCCs found to n_pivot.  Each peel removes at least the root with
 // the largest (or smallest) key, so at most n peels, each with at most n + 1
 // sweeps per fixpoint.
+// With out set the canonical labels of the residual vertices go straight to
+// out and their state words keep the residual tag: the other CTAs are
+// writing every other vertex's label meanwhile, deciding by that tag.
 static __device__ __noinline__ void res_solve(const Graph &g, const Work &w, const uint32_t *L, uint32_t n, const uint32_t *eb,
-                          uint32_t m, Ctl *ctl)
+                          uint32_t m, Ctl *ctl, uint32_t *out = nullptr)
 {
     constexpr uint8_t ALIVE = 1, VIS = 2;
     char *sb = reinterpret_cast<char *>(&sccb_dsmem[BQ_HDR]);
@@ -1283,7 +1286,8 @@ static __device__ __noinline__ void res_solve(const Graph &g, const Work &w, con
     }
     for (uint32_t i = t; i < n; i += T) {
         w.label[gid[i]] = LBL_SELF | aux[col[i]];
-        w.st[gid[i]] = DEAD;
+        if (out) out[gid[i] - 1u] = aux[col[i]];
+        else w.st[gid[i]] = DEAD;
     }
     if (t == 0) {
         atomicAdd(&ctl->n_pivot, (unsigned long long)s_npiv);
