@@ -59,6 +59,7 @@ struct scc_context {
     uint32_t qcap = 320;                 // per-warp staging slice entries (up to 3 queues x 32 warps in shared memory;
                                          // larger slices shrink the L1 data cache and slow the gathers)
     uint32_t bu_k = 2;                   // bottom-up BFS step when frontier edges > bu_k * scope (0 = off)
+    int warp_schedule = 0;               // wHong/wSlota first search: 0 auto, 1 virtual warps, 2 warp walk
     uint32_t pull_lane = 4;              // bottom-up step: list length a lane tests alone (4: 2 % faster
                                          // than 32 on R-MAT scale 22, plain and permuted ids)
     int cluster_check = 0;               // batched launches: bounded software cluster barriers (check mode)

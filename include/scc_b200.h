@@ -144,6 +144,13 @@ int scc_derive_reverse(scc_context *ctx, const uint32_t *Fr, const uint32_t *Fc,
  *   "bu_k"                bottom-up BFS step when the frontier's edges exceed
  *                         bu_k * (vertices the search can reach) (default 2,
  *                         0 = never)
+ *   "warp_schedule"       wHong / wSlota top-down expansion: 0 = the
+ *                         virtual-warp schedule (W lanes per vertex, the
+ *                         reference's fwd_warp<W>) when W > 1 and
+ *                         E >= W * V, else the warp walk of the vertex
+ *                         drivers (default); 1 =
+ *                         always virtual warps; 2 = always the warp walk.
+ *                         Results do not depend on it.
  *   "pull_lane"           bottom-up step: adjacency lists up to this length
  *                         are tested by their lane alone; of a longer list
  *                         the lane tests the first min(8, pull_lane) entries

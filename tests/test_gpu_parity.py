@@ -156,3 +156,28 @@ def test_device_resident_path(engine, oracle_lib):
     lab, counts = _expect(oracle_lib, g, "h", 1, 1)
     assert np.array_equal(out.cpu().numpy().astype(np.uint32), lab)
     assert res.num_sccs == sum(counts)
+
+
+@pytest.mark.parametrize("sched", [1, 2])
+@pytest.mark.parametrize("algo,w", [("x", 1), ("x", 8), ("y", 2), ("y", 8), ("y", 32)])
+def test_warp_schedules(oracle_lib, golden, sched, algo, w):
+    """wHong / wSlota with the virtual-warp schedule forced (1) and the warp
+    walk forced (2): the same labels and counters as the restated reference,
+    on both launch paths (the default picks one by mean degree)."""
+    from detectingscc_b200 import graphs
+    e = scc.Engine(0)
+    e.set_tuning("warp_schedule", sched)
+    try:
+        gs = []
+        for name in SAMPLES:
+            z = golden[name]
+            V = int(z["V"])
+            gs.append(_graph(V, *build_csr(V, z["src"].astype(np.int64), z["dst"].astype(np.int64))))
+        for gen in (lambda: graphs.grid(64, seed=2), lambda: graphs.rmat(12, seed=6)):
+            V, s, d = gen()
+            gs.append(scc.graph_from_arcs(V, s.numpy(), d.numpy()))
+        for g in gs:
+            for force in ("grid", "block"):
+                _check(e, oracle_lib, g, algo, w, 1, 1, force)
+    finally:
+        e.close()
