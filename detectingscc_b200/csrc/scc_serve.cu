@@ -163,7 +163,7 @@ Caps job_caps(const scc_server *s, const Job &j, const Lane *L, bool exact)
     // one scratch slice per CTA, or per cluster for a large graph
     const size_t per = carve_work(nullptr, j.maxV, j.maxE, true, nullptr);
     const size_t slices = j.large ? 1 : job_ctas(s, j);
-    c.S = std::max(L->capScratch, per * slices);
+    c.S = g(L->capScratch, per * slices);
     return c;
 }
 
@@ -550,6 +550,23 @@ extern "C" int scc_server_create(int device, const scc_server_config *cfg, scc_s
     if (cudaMemPoolCreate(&s->pool, &pp) != cudaSuccess) { cudaGetLastError(); delete s; return SCC_ERR_CUDA; }
     unsigned long long keep = ~0ull;
     cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    // A lane's allocation never waits on another lane's stream to reuse
+    // memory that lane freed (such a wait would tie the lanes together).
+    int no = 0;
+    cudaMemPoolSetAttribute(s->pool, cudaMemPoolReuseAllowInternalDependencies, &no);
+    // Reserve memory in the pool up front (1 GiB per lane, at most half the
+    // budget): growing an arena then takes cached memory instead of new
+    // device allocations, which took up to a second under load and stalled
+    // every lane behind them.
+    {
+        const size_t warm = std::min<size_t>((size_t)c.lanes << 30, c.budget_bytes / 2);
+        void *w = nullptr;
+        if (warm && cudaMallocFromPoolAsync(&w, warm, s->pool, 0) == cudaSuccess) {
+            cudaFreeAsync(w, 0);
+            cudaStreamSynchronize(0);
+        }
+        cudaGetLastError();
+    }
     for (uint32_t i = 0; i < c.lanes && rc == SCC_OK; i++) {
         Lane *L = new Lane();
         L->id = (int)i;
