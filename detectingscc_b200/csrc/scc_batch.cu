@@ -71,6 +71,7 @@ __device__ void batch_one(Ex &ex, const BatchParams &p, uint32_t gi, char *base,
         const uint32_t npk = HONG ? 4u * (bg.V + 1u) + 8u : 1u;
         for (uint32_t i = ex.tid(); i < npk; i += ex.nthr()) w.pivkey[i] = 0ull;
         ex.sync();
+        if constexpr (!Ex::cluster) ex.reset_counters();   // this CTA's counter ring and error flag
         if (ex.leader()) {
             w.ctl->timeout_ns = p.timeout_ns;
             w.ctl->first_min = 0xFFFFFFFFu;

@@ -183,8 +183,18 @@ __device__ __forceinline__ unsigned long long gtimer()
     return t;
 }
 __device__ __forceinline__ unsigned vld(const unsigned *p) { return *(const volatile unsigned *)p; }
+// The CTA's own copy of "an error was set", read by the single-CTA
+// barrier instead of the control block's word (one load from L2 less per
+// pass); every set_error raises it.
+__device__ __forceinline__ int *cta_err()
+{
+    __shared__ int s_cta_err;
+    return &s_cta_err;
+}
+
 __device__ __forceinline__ void set_error(Ctl *c, int code, int where)
 {
+    *(volatile int *)cta_err() = 1;
     if (atomicCAS(&c->error, 0, code) == 0) c->where = where;
 }
 
@@ -212,6 +222,14 @@ __device__ __forceinline__ unsigned *cnt_snap()
     __shared__ unsigned s_cnt[NCNT];
     return s_cnt;
 }
+// Pass counter ring of the single-CTA policy (BlockExec): in shared memory,
+// since no other CTA reads it.
+__device__ __forceinline__ unsigned (*block_lc())[NCNT]
+{
+    __shared__ unsigned s_lc[3][NCNT];
+    return s_lc;
+}
+
 __device__ __forceinline__ void take_snap(const unsigned *c)
 {
     unsigned *d = cnt_snap();
@@ -234,6 +252,7 @@ struct GridExec {
     __device__ __forceinline__ unsigned wid() const { return tid() >> 5; }
     __device__ __forceinline__ unsigned nwarps() const { return nthr() >> 5; }
     __device__ __forceinline__ bool leader() const { return blockIdx.x == 0 && threadIdx.x == 0; }
+    __device__ __forceinline__ unsigned *lc(unsigned slot) const { return ctl->lc[slot]; }
 
     // Grid barrier.  One arrival counter: CTA 0 adds 0x80000000 - (n - 1),
     // every other CTA adds 1, so bit 31 flips exactly when all n CTAs have
@@ -296,12 +315,20 @@ struct BlockExec {
     __device__ __forceinline__ unsigned wid() const { return threadIdx.x >> 5; }
     __device__ __forceinline__ unsigned nwarps() const { return blockDim.x >> 5; }
     __device__ __forceinline__ bool leader() const { return threadIdx.x == 0; }
+    __device__ __forceinline__ unsigned *lc(unsigned slot) const { return block_lc()[slot]; }
+    // Counters and the error flag of a new run on this CTA (every thread calls).
+    __device__ void reset_counters() const
+    {
+        for (unsigned i = threadIdx.x; i < 3u * NCNT; i += blockDim.x) (&block_lc()[0][0])[i] = 0u;
+        if (threadIdx.x == 0) *cta_err() = *(volatile int *)&ctl->error != 0;
+        __syncthreads();
+    }
     __device__ bool sync(const unsigned *snap = nullptr)
     {
         __shared__ int s_err;
         __syncthreads();
         if (threadIdx.x == 0) {
-            s_err = *(volatile int *)&ctl->error;
+            s_err = *(volatile int *)cta_err();
             if (snap) take_snap(snap);
         }
         __syncthreads();
@@ -357,6 +384,7 @@ struct ClusterExec {
     __device__ __forceinline__ unsigned wid() const { return tid() >> 5; }
     __device__ __forceinline__ unsigned nwarps() const { return nthr() >> 5; }
     __device__ __forceinline__ bool leader() const { return rank == 0 && threadIdx.x == 0; }
+    __device__ __forceinline__ unsigned *lc(unsigned slot) const { return ctl->lc[slot]; }
     __device__ void barrier()
     {
         if (!soft) {
@@ -421,15 +449,15 @@ __device__ __forceinline__ bool run_pass(Ex &ex, int phase, F &&body)
     const unsigned nxt = ex.gl % 3u, clr = (ex.gl + 1u) % 3u, cur = (ex.gl + 2u) % 3u;
     if (ex.leader()) {
 #pragma unroll
-        for (int i = 0; i < NCNT; i++) ex.ctl->lc[clr][i] = 0u;
+        for (int i = 0; i < NCNT; i++) ex.lc(clr)[i] = 0u;
     }
     body(cur, nxt);
-    bool ok = ex.sync(ex.ctl->lc[nxt]);
+    bool ok = ex.sync(ex.lc(nxt));
     if (ex.leader() && ex.ctl->trace && ex.gl < ex.ctl->trace_cap) {
         // pass trace: end time and (phase, items pushed) -- the reference's
         // _DEBUG per-phase event timers (scc_WCC.cu:650-672) at pass granularity
         // (instrumented runs record the running count of adjacency entries scanned instead)
-        const unsigned *c = ex.ctl->lc[nxt];
+        const unsigned *c = ex.lc(nxt);
         unsigned long long pushed = (unsigned long long)vld(&c[C_FQ]) + vld(&c[C_BQ]) + vld(&c[C_LIST]);
         if constexpr (Ex::instr) pushed = *(volatile unsigned long long *)&ex.ctl->t_edges;
         ex.ctl->trace[2 * ex.gl] = gtimer();
@@ -478,7 +506,10 @@ __device__ __forceinline__ uint32_t *cta_first_min();
 __device__ __forceinline__ void bq_init()
 {
     for (unsigned i = threadIdx.x; i < BQ_HDR; i += blockDim.x) sccb_dsmem[i] = 0u;
-    if (threadIdx.x == 0) *cta_first_min() = 0xFFFFFFFFu;
+    if (threadIdx.x == 0) {
+        *cta_first_min() = 0xFFFFFFFFu;
+        *cta_err() = 0;
+    }
     __syncthreads();
 }
 

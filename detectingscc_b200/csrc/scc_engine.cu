@@ -129,6 +129,7 @@ __global__ void __launch_bounds__(GRID_THREADS, 1) k_scc_grid(Params p)
         if (blockIdx.x != 0) return;
         if (threadIdx.x == 0) { p.w.ctl->tail_pass = cy.gl; p.w.ctl->nlive_tail = cy.nL; }
         BlockExec<INSTR> bx{p.w.ctl, cy.gl, p.pass_cap};
+        bx.reset_counters();
         if (HONG) hong_loop(bx, p.g, p.w, cy, 0u);
         else slota_peels(bx, p.g, p.w, cy, 0u);
         bx.gl = cy.gl;
@@ -151,6 +152,7 @@ __global__ void __launch_bounds__(BLOCK_THREADS, 1) k_scc_block(Params p)
     if (threadIdx.x == 0) p.w.ctl->t_start = gtimer();
     bq_init();
     BlockExec<INSTR> ex{p.w.ctl, 0u, p.pass_cap};
+    ex.reset_counters();
     Carry cy{0u, 0u, 0u};
     int rc = HONG ? hong_front(ex, p.g, p.w, p.t1, p.t2, p.lw, cy) : slota_front(ex, p.g, p.w, p.t1, p.lw, cy);
     if (rc == RUN_DONE) rc = HONG ? hong_loop(ex, p.g, p.w, cy, 0u) : slota_peels(ex, p.g, p.w, cy, 0u);

@@ -218,7 +218,7 @@ __device__ bool ph_init_trim1(Ex &ex, const Graph &g, const Work &w, uint32_t *L
                         best = k > best ? k : best;
                     }
                 }
-                bq_push(0, surv, v, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 10);
+                bq_push(0, surv, v, w.qcap, Lout, &ex.lc(nxt)[C_LIST], g.V, ex.ctl, 10);
             }
             if (i0 + 3u <= g.V) {
                 *reinterpret_cast<uint4 *>(w.st + i0) = make_uint4(st4[0], st4[1], st4[2], st4[3]);
@@ -239,7 +239,7 @@ __device__ bool ph_init_trim1(Ex &ex, const Graph &g, const Work &w, uint32_t *L
         ntrim = __reduce_add_sync(FULL, ntrim);
         if (lane_id() == 0 && ntrim) atomicAdd(&ex.ctl->n_trim1, (unsigned long long)ntrim);
         block_max_atomic(best, &w.pivkey[0]);
-        bq_flush(1, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], nullptr, nullptr, g.V, ex.ctl);
+        bq_flush(1, w.qcap, Lout, &ex.lc(nxt)[C_LIST], nullptr, nullptr, g.V, ex.ctl);
     });
 }
 
@@ -288,8 +288,8 @@ __device__ bool ph_trim1_fix(Ex &ex, const Graph &g, const Work &w, VList src0, 
                     if (v1) u1 = guard_id(u1, g.V, ex.ctl);
                     const bool p0 = v0 && (w.st[u0] & RMASK) == r0 && stamp_claim(w.stamp, u0, tag);
                     const bool p1 = v1 && (w.st[u1] & RMASK) == r1 && stamp_claim(w.stamp, u1, tag);
-                    bq_push(0, p0, u0, w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_FQ], g.V, ex.ctl, 11);
-                    bq_push(0, p1, u1, w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_FQ], g.V, ex.ctl, 11);
+                    bq_push(0, p0, u0, w.qcap, w.Q[0][par], &ex.lc(nxt)[C_FQ], g.V, ex.ctl, 11);
+                    bq_push(0, p1, u1, w.qcap, w.Q[0][par], &ex.lc(nxt)[C_FQ], g.V, ex.ctl, 11);
                 };
 #pragma unroll
                 for (int dir = 0; dir < 2; dir++) {
@@ -300,7 +300,7 @@ __device__ bool ph_trim1_fix(Ex &ex, const Graph &g, const Work &w, VList src0, 
                     count_edges(ex, lbs_expand2(beg, deg, r, C, fn2));
                 }
             }
-            bq_flush(1, w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_FQ], nullptr, nullptr, g.V, ex.ctl);
+            bq_flush(1, w.qcap, w.Q[0][par], &ex.lc(nxt)[C_FQ], nullptr, nullptr, g.V, ex.ctl);
         });
         if (!ok) return false;
         first = false;
@@ -338,9 +338,9 @@ __device__ bool ph_trim2(Ex &ex, const Graph &g, const Work &w, VList src)
             count_verts(ex, valid);
             unsigned m = __ballot_sync(FULL, cnt);
             if (lane_id() == 0 && m) atomicAdd(&ex.ctl->n_trim2, (unsigned long long)__popc(m));
-            bq_push(0, hit, v, w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 12);
+            bq_push(0, hit, v, w.qcap, w.Q[0][par], &ex.lc(nxt)[C_LIST], g.V, ex.ctl, 12);
         }
-        bq_flush(1, w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_LIST], nullptr, nullptr, g.V, ex.ctl);
+        bq_flush(1, w.qcap, w.Q[0][par], &ex.lc(nxt)[C_LIST], nullptr, nullptr, g.V, ex.ctl);
     });
     if (!ok) return false;
     const uint32_t nT = last_count(ex, C_LIST);
@@ -378,7 +378,7 @@ __device__ __forceinline__ void bfs_edge_visit(Ex &ex, const Graph &g, const Wor
     fold_completed(done);
     const uint32_t *Rn = dir ? g.Br : g.Fr;
     bq_add_edges((unsigned)dir, claim ? __ldg(&Rn[nbr + 1]) - __ldg(&Rn[nbr]) : 0u);
-    bq_push((unsigned)dir, claim, nbr, w.qcap, w.Q[dir][par], &ex.ctl->lc[nxt][C_FQ + dir], g.V, ex.ctl, 13);
+    bq_push((unsigned)dir, claim, nbr, w.qcap, w.Q[dir][par], &ex.lc(nxt)[C_FQ + dir], g.V, ex.ctl, 13);
 }
 
 // Two adjacency entries per lane: both gathers and both claims are issued
@@ -405,8 +405,8 @@ __device__ __forceinline__ void bfs_edge_visit2(Ex &ex, const Graph &g, const Wo
     if (c0) e += __ldg(&Rn[n0 + 1]) - __ldg(&Rn[n0]);
     if (c1) e += __ldg(&Rn[n1 + 1]) - __ldg(&Rn[n1]);
     bq_add_edges((unsigned)dir, e);
-    bq_push((unsigned)dir, c0, n0, w.qcap, w.Q[dir][par], &ex.ctl->lc[nxt][C_FQ + dir], g.V, ex.ctl, 13);
-    bq_push((unsigned)dir, c1, n1, w.qcap, w.Q[dir][par], &ex.ctl->lc[nxt][C_FQ + dir], g.V, ex.ctl, 13);
+    bq_push((unsigned)dir, c0, n0, w.qcap, w.Q[dir][par], &ex.lc(nxt)[C_FQ + dir], g.V, ex.ctl, 13);
+    bq_push((unsigned)dir, c1, n1, w.qcap, w.Q[dir][par], &ex.lc(nxt)[C_FQ + dir], g.V, ex.ctl, 13);
 }
 
 template <class Ex>
@@ -420,7 +420,7 @@ __device__ __forceinline__ void bfs_expand_lanes(Ex &ex, const Graph &g, const W
     bool heavy = deg > HEAVY_T;
     uint32_t nch = heavy ? (deg + CH - 1u) / CH : 0u;
     if (lw > 0 && (lane_id() & ((1u << lw) - 1u)) != 0u) nch = 0u;
-    warp_push_chunks(v, nch, w.H[dir][par], &ex.ctl->lc[nxt][C_FH + dir], w.hcap, ex.ctl);
+    warp_push_chunks(v, nch, w.H[dir][par], &ex.lc(nxt)[C_FH + dir], w.hcap, ex.ctl);
     if (heavy) deg = 0u;
     unsigned tot;
     if (lw < 0) {
@@ -457,7 +457,7 @@ __device__ __forceinline__ void bfs_expand_vwk(Ex &ex, const Graph &g, const Wor
     for (int j = 0; j < VWK; j++) {
         const bool heavy = deg[j] > HEAVY_T;
         warp_push_chunks(v[j], heavy && lead ? (deg[j] + CH - 1u) / CH : 0u, w.H[dir][par],
-                         &ex.ctl->lc[nxt][C_FH + dir], w.hcap, ex.ctl);
+                         &ex.lc(nxt)[C_FH + dir], w.hcap, ex.ctl);
         if (heavy) deg[j] = 0u;
     }
     auto fn = [&](int j, bool v0, uint32_t n0, bool v1, uint32_t n1) {
@@ -591,12 +591,12 @@ __device__ __forceinline__ void bfs_pull2(Ex &ex, const Graph &g, const Work &w,
         if (puf) bq_add_edges(0u, found[2 * h] ? __ldg(&g.Fr[v[h] + 1u]) - __ldg(&g.Fr[v[h]]) : 0u);
         if (pub) bq_add_edges(1u, found[2 * h + 1] ? __ldg(&g.Br[v[h] + 1u]) - __ldg(&g.Br[v[h]]) : 0u);
         count_verts(ex, ok[h]);
-        if (puf) bq_push(0u, found[2 * h], v[h], w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_FQ], g.V, ex.ctl, 19);
-        if (pub) bq_push(1u, found[2 * h + 1], v[h], w.qcap, w.Q[1][par], &ex.ctl->lc[nxt][C_BQ], g.V, ex.ctl, 19);
+        if (puf) bq_push(0u, found[2 * h], v[h], w.qcap, w.Q[0][par], &ex.lc(nxt)[C_FQ], g.V, ex.ctl, 19);
+        if (pub) bq_push(1u, found[2 * h + 1], v[h], w.qcap, w.Q[1][par], &ex.lc(nxt)[C_BQ], g.V, ex.ctl, 19);
         if (Ex::nbq > 2 && sout) {
             const bool fv = (s[h] & FVB) || found[2 * h], bv = (s[h] & BVB) || found[2 * h + 1];
             const bool keep = s[h] != DEAD && !(fv && (bv || !bw));
-            bq_push(2u, keep, v[h], w.qcap, sout, &ex.ctl->lc[nxt][C_SCOPE], g.V, ex.ctl, 25);
+            bq_push(2u, keep, v[h], w.qcap, sout, &ex.lc(nxt)[C_SCOPE], g.V, ex.ctl, 25);
         }
     }
     if constexpr (Ex::instr) {
@@ -699,8 +699,8 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
             bfs_expand_lanes(ex, g, w, 0, v, act, r, lw, par, nxt);
             if (bw) bfs_expand_lanes(ex, g, w, 1, v, act, r, lw, par, nxt);
         }
-        bq_flush(2, w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_FQ], w.Q[1][par], &ex.ctl->lc[nxt][C_BQ], g.V, ex.ctl,
-                 &ex.ctl->lc[nxt][C_FE], &ex.ctl->lc[nxt][C_BE]);
+        bq_flush(2, w.qcap, w.Q[0][par], &ex.lc(nxt)[C_FQ], w.Q[1][par], &ex.lc(nxt)[C_BQ], g.V, ex.ctl,
+                 &ex.lc(nxt)[C_FE], &ex.lc(nxt)[C_BE]);
     });
     if (!ok) return false;
     for (unsigned lev = 1;; lev++) {
@@ -776,9 +776,9 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
                     }
                 }
             }
-            bq_flush(sout ? 3u : 2u, w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_FQ], w.Q[1][par],
-                     &ex.ctl->lc[nxt][C_BQ], g.V, ex.ctl, &ex.ctl->lc[nxt][C_FE], &ex.ctl->lc[nxt][C_BE], sout,
-                     &ex.ctl->lc[nxt][C_SCOPE]);
+            bq_flush(sout ? 3u : 2u, w.qcap, w.Q[0][par], &ex.lc(nxt)[C_FQ], w.Q[1][par],
+                     &ex.lc(nxt)[C_BQ], g.V, ex.ctl, &ex.lc(nxt)[C_FE], &ex.lc(nxt)[C_BE], sout,
+                     &ex.lc(nxt)[C_SCOPE]);
         });
         if (!ok) return false;
         if (sout) {   // the next bottom-up steps walk the shrunken scope
@@ -811,7 +811,7 @@ __device__ __forceinline__ void prop_visit(Ex &ex, const Graph &g, const Work &w
             if (s != DEAD && s > c) push = atomicMin(&w.st[u], c) > c && stamp_claim(w.stamp, u, tag);
         }
     }
-    bq_push(0, push, u, w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_FQ], g.V, ex.ctl, 14);
+    bq_push(0, push, u, w.qcap, w.Q[0][par], &ex.lc(nxt)[C_FQ], g.V, ex.ctl, 14);
 }
 
 template <bool MAXP, class Ex>
@@ -854,13 +854,13 @@ __device__ bool ph_propagate(Ex &ex, const Graph &g, const Work &w, VList src0)
                     if (valid) { beg = __ldg(&g.Br[v]); deg = __ldg(&g.Br[v + 1]) - beg; }
                     bool heavy = deg > HEAVY_T;
                     warp_push_chunks(v, heavy ? (deg + CH - 1u) / CH : 0u, w.H[0][par],
-                                     &ex.ctl->lc[nxt][C_FH], w.hcap, ex.ctl);
+                                     &ex.lc(nxt)[C_FH], w.hcap, ex.ctl);
                     if (heavy) deg = 0u;
                     count_verts(ex, valid);
                     count_edges(ex, lbs_expand(beg, deg, c, g.Bc, fn));
                 }
             }
-            bq_flush(1, w.qcap, w.Q[0][par], &ex.ctl->lc[nxt][C_FQ], nullptr, nullptr, g.V, ex.ctl);
+            bq_flush(1, w.qcap, w.Q[0][par], &ex.lc(nxt)[C_FQ], nullptr, nullptr, g.V, ex.ctl);
         });
         if (!ok) return false;
         first = false;
@@ -908,17 +908,17 @@ __device__ bool ph_hong_update(Ex &ex, const Graph &g, const Work &w, VList src,
                 if (single) mn = scc ? min(mn, v[j]) : mn;
                 else smin_fold(scc, p, v[j], w.smin);
                 bq_add_edges(0, surv ? __ldg(&g.Fr[v[j] + 1u]) - __ldg(&g.Fr[v[j]]) : 0u);
-                bq_push(0, surv, v[j], w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 15);
+                bq_push(0, surv, v[j], w.qcap, Lout, &ex.lc(nxt)[C_LIST], g.V, ex.ctl, 15);
                 if (fold) {
                     // the new ranges are listed by their first bid (as in ph_pivots)
                     const bool first = range_max_atomic(surv, nr, surv ? pivot_key(g, v[j]) : 0ull, w.pivkey);
-                    warp_push(first, nr, w.Q[0][ex.gl & 1u], &ex.ctl->lc[nxt][C_RNG], g.V + 1u, ex.ctl, 22);
+                    warp_push(first, nr, w.Q[0][ex.gl & 1u], &ex.lc(nxt)[C_RNG], g.V + 1u, ex.ctl, 22);
                 }
             }
             count_verts_n(ex, (unsigned)ok[0] + ok[1] + ok[2] + ok[3]);
         }
         if (single) block_min_atomic(mn, w.pivkey[0] ? &w.smin[key_vertex(w.pivkey[0])] : w.smin);
-        bq_flush(1, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], nullptr, nullptr, g.V, ex.ctl, &ex.ctl->lc[nxt][C_FE]);
+        bq_flush(1, w.qcap, Lout, &ex.lc(nxt)[C_LIST], nullptr, nullptr, g.V, ex.ctl, &ex.lc(nxt)[C_FE]);
     });
 }
 
@@ -946,12 +946,12 @@ __device__ bool ph_slota_first_update(Ex &ex, const Graph &g, const Work &w, VLi
                 }
                 mn = scc ? min(mn, v[j]) : mn;
                 bq_add_edges(0, surv ? __ldg(&g.Fr[v[j] + 1u]) - __ldg(&g.Fr[v[j]]) : 0u);
-                bq_push(0, surv, v[j], w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 16);
+                bq_push(0, surv, v[j], w.qcap, Lout, &ex.lc(nxt)[C_LIST], g.V, ex.ctl, 16);
             }
             count_verts_n(ex, (unsigned)ok[0] + ok[1] + ok[2] + ok[3]);
         }
         block_min_atomic(mn, w.pivkey[0] ? &w.smin[p] : w.smin);   // mn stays 0xFFFFFFFF without a pivot
-        bq_flush(1, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], nullptr, nullptr, g.V, ex.ctl, &ex.ctl->lc[nxt][C_FE]);
+        bq_flush(1, w.qcap, Lout, &ex.lc(nxt)[C_LIST], nullptr, nullptr, g.V, ex.ctl, &ex.lc(nxt)[C_FE]);
     });
 }
 
@@ -976,13 +976,13 @@ __device__ bool ph_slota_first_update_lazy(Ex &ex, const Graph &g, const Work &w
                 const bool surv = s[j] != DEAD && (s[j] & (FVB | BVB)) != (FVB | BVB);
                 if (surv) { w.st[v[j]] = v[j]; w.stamp[v[j]] = 0u; }
                 bq_add_edges(0, surv ? __ldg(&g.Fr[v[j] + 1u]) - __ldg(&g.Fr[v[j]]) : 0u);
-                bq_push(0, surv, v[j], w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 16);
+                bq_push(0, surv, v[j], w.qcap, Lout, &ex.lc(nxt)[C_LIST], g.V, ex.ctl, 16);
             }
             count_verts_n(ex, (unsigned)ok[0] + ok[1] + ok[2] + ok[3]);
         }
         __syncthreads();
         if (threadIdx.x == 0 && *cta_first_min() != 0xFFFFFFFFu) atomicMin(&ex.ctl->first_min, *cta_first_min());
-        bq_flush(1, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], nullptr, nullptr, g.V, ex.ctl, &ex.ctl->lc[nxt][C_FE]);
+        bq_flush(1, w.qcap, Lout, &ex.lc(nxt)[C_LIST], nullptr, nullptr, g.V, ex.ctl, &ex.lc(nxt)[C_FE]);
     });
 }
 
@@ -1009,11 +1009,11 @@ __device__ bool ph_slota_peel_update(Ex &ex, const Graph &g, const Work &w, VLis
                 }
                 smin_fold(scc, c, v[j], w.smin);
                 bq_add_edges(0, surv ? __ldg(&g.Fr[v[j] + 1u]) - __ldg(&g.Fr[v[j]]) : 0u);
-                bq_push(0, surv, v[j], w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 17);
+                bq_push(0, surv, v[j], w.qcap, Lout, &ex.lc(nxt)[C_LIST], g.V, ex.ctl, 17);
             }
             count_verts_n(ex, (unsigned)ok[0] + ok[1] + ok[2] + ok[3]);
         }
-        bq_flush(1, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], nullptr, nullptr, g.V, ex.ctl, &ex.ctl->lc[nxt][C_FE]);
+        bq_flush(1, w.qcap, Lout, &ex.lc(nxt)[C_LIST], nullptr, nullptr, g.V, ex.ctl, &ex.lc(nxt)[C_FE]);
     });
 }
 
@@ -1034,11 +1034,11 @@ __device__ bool ph_compact_rename(Ex &ex, const Graph &g, const Work &w, VList s
             for (int j = 0; j < 4; j++) {
                 const bool surv = s[j] != DEAD;
                 if (surv) w.st[v[j]] = v[j];
-                bq_push(0, surv, v[j], w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 18);
+                bq_push(0, surv, v[j], w.qcap, Lout, &ex.lc(nxt)[C_LIST], g.V, ex.ctl, 18);
             }
             count_verts_n(ex, (unsigned)ok[0] + ok[1] + ok[2] + ok[3]);
         }
-        bq_flush(1, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], nullptr, nullptr, g.V, ex.ctl);
+        bq_flush(1, w.qcap, Lout, &ex.lc(nxt)[C_LIST], nullptr, nullptr, g.V, ex.ctl);
     });
 }
 
@@ -1056,10 +1056,10 @@ __device__ bool ph_pivots(Ex &ex, const Graph &g, const Work &w, VList src)
             uint32_t v = valid ? src.at(i) : 0u;
             uint32_t r = valid ? (w.st[v] & RMASK) : 0u;
             const bool first = range_max_atomic(valid, r, valid ? pivot_key(g, v) : 0ull, w.pivkey);
-            warp_push(first, r, w.Q[0][par], &ex.ctl->lc[nxt][C_RNG], g.V + 1u, ex.ctl, 21);
+            warp_push(first, r, w.Q[0][par], &ex.lc(nxt)[C_RNG], g.V + 1u, ex.ctl, 21);
             bq_add_edges(0, valid ? __ldg(&g.Fr[v + 1u]) - __ldg(&g.Fr[v]) : 0u);
         }
-        bq_flush_edges(&ex.ctl->lc[nxt][C_FE]);   // out-arcs of the live list (the residual check)
+        bq_flush_edges(&ex.lc(nxt)[C_FE]);   // out-arcs of the live list (the residual check)
     });
 }
 
@@ -1172,7 +1172,7 @@ __device__ bool res_extract(Ex &ex, const Graph &g, const Work &w, Carry &cy)
                     hit = (s & (FVB | BVB)) == (FVB | BVB) && (s & RMASK) != 0u;
                     e = (src << 16) | ((s & RMASK) - 1u);
                 }
-                warp_push(hit, e, eb, &ex.ctl->lc[nxt][C_BQ], RES_MAX_E, ex.ctl, 24);
+                warp_push(hit, e, eb, &ex.lc(nxt)[C_BQ], RES_MAX_E, ex.ctl, 24);
             };
             count_edges(ex, lbs_expand(beg, deg, i, g.Fc, fn));
         }
@@ -1369,12 +1369,12 @@ __device__ bool ph_first_pivot(Ex &ex, const Graph &g, const Work &w, uint32_t *
                     unsigned long long k = pivot_key(g, v);
                     best = k > best ? k : best;
                 }
-                bq_push(0, live, v, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], g.V, ex.ctl, 20);
+                bq_push(0, live, v, w.qcap, Lout, &ex.lc(nxt)[C_LIST], g.V, ex.ctl, 20);
             }
             count_verts_n(ex, i0 <= g.V ? min(4u, g.V + 1u - i0) : 0u);
         }
         block_max_atomic(best, &w.pivkey[0]);
-        bq_flush(1, w.qcap, Lout, &ex.ctl->lc[nxt][C_LIST], nullptr, nullptr, g.V, ex.ctl);
+        bq_flush(1, w.qcap, Lout, &ex.lc(nxt)[C_LIST], nullptr, nullptr, g.V, ex.ctl);
     });
 }
 
