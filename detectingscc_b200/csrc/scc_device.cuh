@@ -53,7 +53,9 @@ struct __align__(128) Ctl {
     unsigned bar_count;
     int error;
     int where; unsigned _p0[29];
-    unsigned lc[3][NCNT]; unsigned _p3[5];         // per-pass counters, 3-slot ring
+    unsigned lc[3][NCNT];                          // per-pass counters, 3-slot ring
+    unsigned maxdeg;                               // largest out- or in-degree (init sweep)
+    unsigned _p3[4];
     unsigned long long n_trim1, n_trim2, n_pivot;
     unsigned long long t_edges, t_verts;           // instrumented work counters
     unsigned passes, outer;                        // passes run, peels / iterations
@@ -813,17 +815,37 @@ __device__ __forceinline__ void block_min_atomic(uint32_t x, uint32_t *dst)
     __syncthreads();
 }
 
+// 32-bit max over the warp, then the CTA; the CTA's thread 0 performs one
+// atomicMax.  Called by every thread of the CTA.
+__device__ __forceinline__ void block_max_atomic32(uint32_t x, uint32_t *dst)
+{
+    __shared__ uint32_t s_max[32];
+    const uint32_t m = __reduce_max_sync(FULL, x);
+    const unsigned wi = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (lane_id() == 0) s_max[wi] = m;
+    __syncthreads();
+    if (wi == 0) {
+        const uint32_t r = __reduce_max_sync(FULL, lane_id() < nw ? s_max[lane_id()] : 0u);
+        if (lane_id() == 0 && r > *(volatile uint32_t *)dst) atomicMax(dst, r);
+    }
+    __syncthreads();
+}
+
 // 64-bit max of a pivot key over the warp, then the CTA; the CTA's thread 0
-// performs one atomicMax.  Called by every thread of the CTA.
-__device__ __forceinline__ void block_max_atomic(unsigned long long key, unsigned long long *dst)
+// performs one atomicMax.  With dst32 set, the 32-bit max of x goes to
+// dst32 in the same two barriers.  Called by every thread of the CTA.
+__device__ __forceinline__ void block_max_atomic(unsigned long long key, unsigned long long *dst, uint32_t x = 0u,
+                                                 uint32_t *dst32 = nullptr)
 {
     __shared__ unsigned long long s_red[32];
+    __shared__ uint32_t s_x[32];
     unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
     unsigned mhi = __reduce_max_sync(FULL, hi);
     unsigned mlo = __reduce_max_sync(FULL, hi == mhi ? lo : 0u);
     unsigned long long wk = ((unsigned long long)mhi << 32) | mlo;
     unsigned w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    if (lane_id() == 0) s_red[w] = wk;
+    const uint32_t mx = dst32 ? __reduce_max_sync(FULL, x) : 0u;
+    if (lane_id() == 0) { s_red[w] = wk; s_x[w] = mx; }
     __syncthreads();
     if (w == 0) {
         const unsigned long long k = lane_id() < nw ? s_red[lane_id()] : 0ull;
@@ -831,6 +853,10 @@ __device__ __forceinline__ void block_max_atomic(unsigned long long key, unsigne
         const unsigned klo = __reduce_max_sync(FULL, (unsigned)(k >> 32) == khi ? (unsigned)k : 0u);
         const unsigned long long m = ((unsigned long long)khi << 32) | klo;
         if (lane_id() == 0 && m && m > *(volatile unsigned long long *)dst) atomicMax(dst, m);
+        if (dst32) {
+            const uint32_t r = __reduce_max_sync(FULL, lane_id() < nw ? s_x[lane_id()] : 0u);
+            if (lane_id() == 0 && r > *(volatile uint32_t *)dst32) atomicMax(dst32, r);
+        }
     }
     __syncthreads();
 }

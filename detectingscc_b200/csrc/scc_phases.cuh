@@ -134,6 +134,7 @@ __device__ bool ph_init(Ex &ex, const Graph &g, const Work &w, bool fold_pivot)
                             g.Fr[g.V + 1] != g.E || g.Br[g.V + 1] != g.E))
             set_error(ex.ctl, E_BAD_GRAPH, 62);
         bool bad = false;
+        uint32_t dmax = 0;
         for (uint32_t i0 = ex.tid() * 4u; i0 <= g.V; i0 += ex.nthr() * 4u) {
             uint32_t f[5], b[5];
             load_off5(g.Fr, i0, g.V, g.vec, f);
@@ -143,6 +144,7 @@ __device__ bool ph_init(Ex &ex, const Graph &g, const Work &w, bool fold_pivot)
                 const uint32_t i = i0 + (uint32_t)j;
                 if (i <= g.V) {
                     bad |= f[j] > f[j + 1] || b[j] > b[j + 1];
+                    dmax = max(dmax, max(f[j + 1] - f[j], b[j + 1] - b[j]));
                     if (fold_pivot && i != 0u) {
                         unsigned long long k = ((unsigned long long)((f[j + 1] - f[j]) * (b[j + 1] - b[j])) << 32) |
                                                (0xFFFFFFFFu - i);
@@ -161,7 +163,8 @@ __device__ bool ph_init(Ex &ex, const Graph &g, const Work &w, bool fold_pivot)
             }
         }
         if (bad) set_error(ex.ctl, E_BAD_GRAPH, 61);
-        if (fold_pivot) block_max_atomic(best, &w.pivkey[0]);
+        if (fold_pivot) block_max_atomic(best, &w.pivkey[0], dmax, &ex.ctl->maxdeg);
+        else block_max_atomic32(dmax, &ex.ctl->maxdeg);
     });
 }
 
@@ -187,6 +190,7 @@ __device__ bool ph_init_trim1(Ex &ex, const Graph &g, const Work &w, uint32_t *L
         unsigned long long best = 0;
         unsigned ntrim = 0;
         bool bad = false;
+        uint32_t dmax = 0;
         for (uint32_t base = ex.wid() * 128u; base <= g.V; base += ex.nwarps() * 128u) {
             const uint32_t i0 = base + 4u * lane_id();
             uint32_t f[5], b[5];
@@ -208,6 +212,7 @@ __device__ bool ph_init_trim1(Ex &ex, const Graph &g, const Work &w, uint32_t *L
                 if (v <= g.V) bad |= f[j] > f[j + 1] || b[j] > b[j + 1];
                 if (valid) {
                     const uint32_t indeg = b[j + 1] - b[j], outdeg = f[j + 1] - f[j];
+                    dmax = max(dmax, max(indeg, outdeg));
                     if (indeg == 0u || outdeg == 0u) {
                         lb4[j] = v | LBL_SELF;   // a trimmed vertex is its own SCC
                         ntrim++;
@@ -238,7 +243,7 @@ __device__ bool ph_init_trim1(Ex &ex, const Graph &g, const Work &w, uint32_t *L
         if (bad) set_error(ex.ctl, E_BAD_GRAPH, 61);
         ntrim = __reduce_add_sync(FULL, ntrim);
         if (lane_id() == 0 && ntrim) atomicAdd(&ex.ctl->n_trim1, (unsigned long long)ntrim);
-        block_max_atomic(best, &w.pivkey[0]);
+        block_max_atomic(best, &w.pivkey[0], dmax, &ex.ctl->maxdeg);
         bq_flush(1, w.qcap, Lout, &ex.lc(nxt)[C_LIST], nullptr, nullptr, g.V, ex.ctl);
     });
 }
@@ -361,7 +366,7 @@ __device__ bool ph_trim2(Ex &ex, const Graph &g, const Work &w, VList src)
 // ---------------------------------------------------------------------
 template <class Ex>
 __device__ __forceinline__ void bfs_edge_visit(Ex &ex, const Graph &g, const Work &w, int dir, bool valid,
-                                               uint32_t nbr, uint32_t r, unsigned par, unsigned nxt)
+                                               uint32_t nbr, uint32_t r, unsigned par, unsigned nxt, bool cnt)
 {
     const uint32_t bit = dir ? BVB : FVB;
     bool claim = false;
@@ -377,16 +382,19 @@ __device__ __forceinline__ void bfs_edge_visit(Ex &ex, const Graph &g, const Wor
     }
     fold_completed(done);
     const uint32_t *Rn = dir ? g.Br : g.Fr;
-    bq_add_edges((unsigned)dir, claim ? __ldg(&Rn[nbr + 1]) - __ldg(&Rn[nbr]) : 0u);
+    if (cnt) bq_add_edges((unsigned)dir, claim ? __ldg(&Rn[nbr + 1]) - __ldg(&Rn[nbr]) : 0u);
     bq_push((unsigned)dir, claim, nbr, w.qcap, w.Q[dir][par], &ex.lc(nxt)[C_FQ + dir], g.V, ex.ctl, 13);
 }
 
 // Two adjacency entries per lane: both gathers and both claims are issued
-// before either append, so every lane keeps two requests in flight.
+// before either append, so every lane keeps two requests in flight.  cnt
+// (uniform over the CTA) adds the claimed vertices' degrees to the pass's
+// frontier-edge tally; a pass whose claims cannot reach the bottom-up
+// threshold skips those offset gathers.
 template <class Ex>
 __device__ __forceinline__ void bfs_edge_visit2(Ex &ex, const Graph &g, const Work &w, int dir, bool v0, uint32_t n0,
                                                 uint32_t r0, bool v1, uint32_t n1, uint32_t r1, unsigned par,
-                                                unsigned nxt)
+                                                unsigned nxt, bool cnt)
 {
     const uint32_t bit = dir ? BVB : FVB;
     if (v0) n0 = guard_id(n0, g.V, ex.ctl);
@@ -400,18 +408,21 @@ __device__ __forceinline__ void bfs_edge_visit2(Ex &ex, const Graph &g, const Wo
     const bool c0 = !(o0 & bit), c1 = !(o1 & bit);
     fold_completed(min(c0 ? completed(o0, bit, n0) : 0xFFFFFFFFu, c1 ? completed(o1, bit, n1) : 0xFFFFFFFFu));
     // edges the claimed vertices will expand next (direction-switch rule)
-    const uint32_t *Rn = dir ? g.Br : g.Fr;
-    unsigned e = 0;
-    if (c0) e += __ldg(&Rn[n0 + 1]) - __ldg(&Rn[n0]);
-    if (c1) e += __ldg(&Rn[n1 + 1]) - __ldg(&Rn[n1]);
-    bq_add_edges((unsigned)dir, e);
+    if (cnt) {
+        const uint32_t *Rn = dir ? g.Br : g.Fr;
+        unsigned e = 0;
+        if (c0) e += __ldg(&Rn[n0 + 1]) - __ldg(&Rn[n0]);
+        if (c1) e += __ldg(&Rn[n1 + 1]) - __ldg(&Rn[n1]);
+        bq_add_edges((unsigned)dir, e);
+    }
     bq_push((unsigned)dir, c0, n0, w.qcap, w.Q[dir][par], &ex.lc(nxt)[C_FQ + dir], g.V, ex.ctl, 13);
     bq_push((unsigned)dir, c1, n1, w.qcap, w.Q[dir][par], &ex.lc(nxt)[C_FQ + dir], g.V, ex.ctl, 13);
 }
 
 template <class Ex>
 __device__ __forceinline__ void bfs_expand_lanes(Ex &ex, const Graph &g, const Work &w, int dir, uint32_t v,
-                                                 bool act, uint32_t r, int lw, unsigned par, unsigned nxt)
+                                                 bool act, uint32_t r, int lw, unsigned par, unsigned nxt,
+                                                 bool cnt = true)
 {
     const uint32_t *R = dir ? g.Br : g.Fr;
     const uint32_t *C = dir ? g.Bc : g.Fc;
@@ -425,11 +436,13 @@ __device__ __forceinline__ void bfs_expand_lanes(Ex &ex, const Graph &g, const W
     unsigned tot;
     if (lw < 0) {
         auto fn2 = [&](bool v0, uint32_t n0, uint32_t r0, bool v1, uint32_t n1, uint32_t r1) {
-            bfs_edge_visit2(ex, g, w, dir, v0, n0, r0, v1, n1, r1, par, nxt);
+            bfs_edge_visit2(ex, g, w, dir, v0, n0, r0, v1, n1, r1, par, nxt, cnt);
         };
         tot = lbs_expand2(beg, deg, r, C, fn2);
     } else {
-        auto fn = [&](bool valid, uint32_t nbr, uint32_t rr) { bfs_edge_visit(ex, g, w, dir, valid, nbr, rr, par, nxt); };
+        auto fn = [&](bool valid, uint32_t nbr, uint32_t rr) {
+            bfs_edge_visit(ex, g, w, dir, valid, nbr, rr, par, nxt, cnt);
+        };
         tot = vw_expand(beg, deg, r, (unsigned)lw, C, fn);
     }
     count_edges(ex, tot);
@@ -442,7 +455,8 @@ constexpr int VWK = 4;
 template <class Ex>
 __device__ __forceinline__ void bfs_expand_vwk(Ex &ex, const Graph &g, const Work &w, int dir,
                                                const uint32_t (&v)[VWK], const bool (&act)[VWK],
-                                               const uint32_t (&r)[VWK], int lw, unsigned par, unsigned nxt)
+                                               const uint32_t (&r)[VWK], int lw, unsigned par, unsigned nxt,
+                                               bool cnt)
 {
     const uint32_t *R = dir ? g.Br : g.Fr;
     const uint32_t *C = dir ? g.Bc : g.Fc;
@@ -461,7 +475,7 @@ __device__ __forceinline__ void bfs_expand_vwk(Ex &ex, const Graph &g, const Wor
         if (heavy) deg[j] = 0u;
     }
     auto fn = [&](int j, bool v0, uint32_t n0, bool v1, uint32_t n1) {
-        bfs_edge_visit2(ex, g, w, dir, v0, n0, r[j], v1, n1, r[j + 1], par, nxt);
+        bfs_edge_visit2(ex, g, w, dir, v0, n0, r[j], v1, n1, r[j + 1], par, nxt, cnt);
     };
     count_edges(ex, vw_expandK<VWK>(beg, deg, (unsigned)lw, C, fn));
 }
@@ -671,7 +685,7 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
                 const uint32_t e0 = beg + lane_id(), e1 = e0 + 32u;
                 const bool v0 = e0 < end, v1 = e1 < end;
                 const uint32_t n0 = v0 ? __ldg(&C[e0]) : 0u, n1 = v1 ? __ldg(&C[e1]) : 0u;
-                bfs_edge_visit2(ex, g, w, dir, v0, n0, r, v1, n1, r, par, nxt);
+                bfs_edge_visit2(ex, g, w, dir, v0, n0, r, v1, n1, r, par, nxt, true);
                 count_edges(ex, end - beg);
             }
         }
@@ -703,6 +717,13 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
                  &ex.lc(nxt)[C_FE], &ex.lc(nxt)[C_BE]);
     });
     if (!ok) return false;
+    // The claims of a pass are tallied by degree (the frontier edges Beamer's
+    // rule weighs) only while they could reach the bottom-up threshold: a
+    // pass claims at most the edges it expands (and at most the scope), and
+    // each claim brings at most maxdeg edges.  Bit d of known: the previous
+    // pass tallied direction d, so its count is exact.
+    unsigned known = 3u;
+    const uint32_t dmax32 = __ldcg(&ex.ctl->maxdeg);
     for (unsigned lev = 1;; lev++) {
         const uint32_t nf = last_count(ex, C_FQ), nb = last_count(ex, C_BQ);
         const uint32_t nhf = last_count(ex, C_FH), nhb = last_count(ex, C_BH);
@@ -716,6 +737,22 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
         const uint32_t mf = last_count(ex, C_FE), mb = last_count(ex, C_BE);
         const bool puf = w.bu_k && (unsigned long long)mf > (unsigned long long)scope.n * w.bu_k;
         const bool pub = bw && w.bu_k && (unsigned long long)mb > (unsigned long long)scope.n * w.bu_k;
+        unsigned cm = 0u;   // bit d: this pass tallies direction d
+        {
+            const unsigned long long dmax = dmax32;
+#pragma unroll
+            for (int d = 0; d < 2; d++) {
+                const bool pu = d ? pub : puf;
+                const unsigned long long nfd = d ? nb : nf, mfd = d ? mb : mf, nhd = d ? nhb : nhf;
+                unsigned long long xe = pu ? scope.n : (((known >> d) & 1u) ? mfd : nfd * dmax) + nhd * CH;
+                xe = min(xe, (unsigned long long)scope.n);
+                if (w.bu_k && xe * dmax > (unsigned long long)scope.n * w.bu_k) cm |= 1u << d;
+            }
+            // a bottom-up step may shrink the scope the next pass weighs
+            // against, so it tallies both directions (and its finds)
+            if (puf || pub) cm = 3u;
+            known = cm;
+        }
         // bottom-up steps (both directions in one sweep of 64-vertex items)
         // walk the ids instead of the scope list when it holds most of them
         const VList psrc = 2ull * scope.n >= (unsigned long long)g.V ? VList{nullptr, g.V, 1u} : scope;
@@ -743,7 +780,7 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
                     uint2 hc = w.H[dir][cp][k];
                     uint32_t r = w.st[hc.x] & RMASK;
                     auto fn2 = [&](bool v0, uint32_t n0, uint32_t r0, bool v1, uint32_t n1, uint32_t r1) {
-                        bfs_edge_visit2(ex, g, w, dir, v0, n0, r0, v1, n1, r1, par, nxt);
+                        bfs_edge_visit2(ex, g, w, dir, v0, n0, r0, v1, n1, r1, par, nxt, (cm >> dir) & 1u);
                     };
                     chunk_expand(ex, dir ? g.Br : g.Fr, dir ? g.Bc : g.Fc, hc, r, fn2);
                 } else {
@@ -757,7 +794,7 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
                     bool lead = (lw <= 0) || ((lane_id() & ((1u << lw) - 1u)) == 0u);
                     if (lw < 0) {
                         count_verts(ex, valid && lead);
-                        bfs_expand_lanes(ex, g, w, dir, v, valid, r, lw, par, nxt);
+                        bfs_expand_lanes(ex, g, w, dir, v, valid, r, lw, par, nxt, (cm >> dir) & 1u);
                     } else {
                         uint32_t vk[VWK], rk[VWK];
                         bool ak[VWK];
@@ -772,7 +809,7 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
                             rk[j] = ak[j] ? (w.st[vk[j]] & RMASK) : 0u;
                             count_verts(ex, ak[j] && lead);
                         }
-                        bfs_expand_vwk(ex, g, w, dir, vk, ak, rk, lw, par, nxt);
+                        bfs_expand_vwk(ex, g, w, dir, vk, ak, rk, lw, par, nxt, (cm >> dir) & 1u);
                     }
                 }
             }

@@ -181,3 +181,26 @@ def test_warp_schedules(oracle_lib, golden, sched, algo, w):
                 _check(e, oracle_lib, g, algo, w, 1, 1, force)
     finally:
         e.close()
+
+
+@pytest.mark.parametrize("algo,w", [("h", 1), ("y", 8), ("g", 1)])
+def test_direction_rule(oracle_lib, algo, w):
+    """The frontier-edge tally behind the bottom-up rule is skipped on passes
+    whose claims cannot reach the threshold (claims x maximum degree): labels
+    and counters match the restated reference with bottom-up steps allowed
+    and switched off, R-MAT still takes bottom-up steps on the whole-GPU
+    kernel, and the low-degree grid takes none."""
+    from detectingscc_b200 import graphs
+    e = scc.Engine(0)
+    e.set_tuning("trace", 4096)
+    try:
+        for gen, hubs in ((lambda: graphs.rmat(16, seed=4), True), (lambda: graphs.grid(192, seed=5), False)):
+            V, s, d = gen()
+            g = scc.graph_from_arcs(V, s.numpy(), d.numpy())
+            for bu in (2, 0):
+                e.set_tuning("bu_k", bu)
+                _check(e, oracle_lib, g, algo, w, 1, 1, "grid")
+                pulled = any(p == "bfs_pull" for p, _, _ in e.trace())
+                assert pulled == (hubs and bu > 0), (algo, w, bu, hubs)
+    finally:
+        e.close()
