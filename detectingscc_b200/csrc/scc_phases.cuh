@@ -163,8 +163,8 @@ __device__ bool ph_init(Ex &ex, const Graph &g, const Work &w, bool fold_pivot)
             }
         }
         if (bad) set_error(ex.ctl, E_BAD_GRAPH, 61);
-        if (fold_pivot) block_max_atomic(best, &w.pivkey[0], dmax, &ex.ctl->maxdeg);
-        else block_max_atomic32(dmax, &ex.ctl->maxdeg);
+        if (fold_pivot) block_max_atomic(best, &w.pivkey[0], dmax, Ex::nbq > 2 ? &ex.ctl->maxdeg : nullptr);
+        else if constexpr (Ex::nbq > 2) block_max_atomic32(dmax, &ex.ctl->maxdeg);
     });
 }
 
@@ -243,7 +243,7 @@ __device__ bool ph_init_trim1(Ex &ex, const Graph &g, const Work &w, uint32_t *L
         if (bad) set_error(ex.ctl, E_BAD_GRAPH, 61);
         ntrim = __reduce_add_sync(FULL, ntrim);
         if (lane_id() == 0 && ntrim) atomicAdd(&ex.ctl->n_trim1, (unsigned long long)ntrim);
-        block_max_atomic(best, &w.pivkey[0], dmax, &ex.ctl->maxdeg);
+        block_max_atomic(best, &w.pivkey[0], dmax, Ex::nbq > 2 ? &ex.ctl->maxdeg : nullptr);
         bq_flush(1, w.qcap, Lout, &ex.lc(nxt)[C_LIST], nullptr, nullptr, g.V, ex.ctl);
     });
 }
@@ -721,9 +721,12 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
     // rule weighs) only while they could reach the bottom-up threshold: a
     // pass claims at most the edges it expands (and at most the scope), and
     // each claim brings at most maxdeg edges.  Bit d of known: the previous
-    // pass tallied direction d, so its count is exact.
+    // pass tallied direction d, so its count is exact.  Whole-GPU policy
+    // only: the single-CTA and batched searches are short, and there the
+    // extra registers cost more than the gathers they save.
+    constexpr bool skip_tally = Ex::nbq > 2;
     unsigned known = 3u;
-    const uint32_t dmax32 = __ldcg(&ex.ctl->maxdeg);
+    const uint32_t dmax32 = skip_tally ? __ldcg(&ex.ctl->maxdeg) : 0u;
     for (unsigned lev = 1;; lev++) {
         const uint32_t nf = last_count(ex, C_FQ), nb = last_count(ex, C_BQ);
         const uint32_t nhf = last_count(ex, C_FH), nhb = last_count(ex, C_BH);
@@ -737,8 +740,9 @@ __device__ bool ph_bfs(Ex &ex, const Graph &g, const Work &w, VList src, Seed se
         const uint32_t mf = last_count(ex, C_FE), mb = last_count(ex, C_BE);
         const bool puf = w.bu_k && (unsigned long long)mf > (unsigned long long)scope.n * w.bu_k;
         const bool pub = bw && w.bu_k && (unsigned long long)mb > (unsigned long long)scope.n * w.bu_k;
-        unsigned cm = 0u;   // bit d: this pass tallies direction d
-        {
+        unsigned cm = 3u;   // bit d: this pass tallies direction d
+        if constexpr (skip_tally) {
+            cm = 0u;
             const unsigned long long dmax = dmax32;
 #pragma unroll
             for (int d = 0; d < 2; d++) {
